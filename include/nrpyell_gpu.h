@@ -1,0 +1,176 @@
+/*
+ * nrpyell_gpu.h -- C ABI of the B200 (sm_100a) hyperbolic-relaxation library.
+ *
+ * Part 1 keeps the reference prototypes of NRPyElliptic's hot path, so the
+ * reference main.c links against libnrpyell_gpu.so unchanged.  Part 2 adds
+ * set-up helpers, a stop-on-tolerance relaxation driver and the mixed
+ * precision / batched drivers.  All gridfunction pointers handed to Part 1
+ * and to the device drivers must be device-accessible (memory from the
+ * allocators below, cudaMalloc or cudaMallocManaged); plain host memory is
+ * rejected with an error, never dereferenced on the GPU.
+ *
+ * Errors: every CUDA call is checked.  By default an error prints
+ * "file:line message" to stderr and calls exit(1), the reference's
+ * convention for set-up failures; nrpyell_set_exit_on_error(0) turns that
+ * into a recorded status (nrpyell_last_status / nrpyell_last_error).
+ *
+ * Threading: one host thread, one CUDA stream per process; calls run in
+ * program order on that stream.  L2_norm_of_gf is the only Part-1 call that
+ * waits for the GPU (it returns a host scalar).
+ */
+#ifndef NRPYELL_GPU_H
+#define NRPYELL_GPU_H
+
+#include <stddef.h>
+#include "nrpyell_abi.h"
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---------------- Part 1: reference prototypes ---------------- */
+
+/* Replaces MoL_malloc_y_n_gfs.c:7-14 (NRPy_function_prototypes.h:1): y_n_gfs in
+ * CUDA managed memory, so host set-up code can still write it. */
+void MoL_malloc_y_n_gfs(const paramstruct *NRPYELL_RESTRICT params, MoL_gridfunctions_struct *NRPYELL_RESTRICT gridfuncs);
+/* Replaces MoL_free_memory_y_n_gfs.c:7-11. */
+void MoL_free_memory_y_n_gfs(const paramstruct *NRPYELL_RESTRICT params, MoL_gridfunctions_struct *NRPYELL_RESTRICT gridfuncs);
+/* Replaces MoL_malloc_non_y_n_gfs.c:7-17; diagnostic_output_gfs aliases
+ * y_nplus1_running_total_gfs exactly as in the reference. */
+void MoL_malloc_non_y_n_gfs(const paramstruct *NRPYELL_RESTRICT params, MoL_gridfunctions_struct *NRPYELL_RESTRICT gridfuncs);
+/* Replaces MoL_free_memory_non_y_n_gfs.c:7-14. */
+void MoL_free_memory_non_y_n_gfs(const paramstruct *NRPYELL_RESTRICT params, MoL_gridfunctions_struct *NRPYELL_RESTRICT gridfuncs);
+
+/* Replaces MoL_step_forward_in_time.c:7-178: one RK4 step of (uu,vv). */
+void MoL_step_forward_in_time(griddata_struct *NRPYELL_RESTRICT griddata, const REAL dt);
+
+/* Replaces rhs_eval.c:7-117: interior RHS of (uu,vv); bitwise the reference's
+ * operation order (every FMA, product and quotient as in rhs_eval.c:86-112). */
+void rhs_eval(const paramstruct *NRPYELL_RESTRICT params, const rfm_struct *NRPYELL_RESTRICT rfmstruct,
+              const REAL *NRPYELL_RESTRICT auxevol_gfs, const REAL *NRPYELL_RESTRICT in_gfs, REAL *NRPYELL_RESTRICT rhs_gfs);
+
+/* Replaces apply_bcs_outerradiation_and_inner.c:410-469: radiation BC on the
+ * RHS at pure outer points, layer by layer, then the inner parity copy. */
+void apply_bcs_outerradiation_and_inner(const paramstruct *NRPYELL_RESTRICT params, const bc_struct *NRPYELL_RESTRICT bcstruct,
+                                        REAL *NRPYELL_RESTRICT xx[3], const REAL custom_wavespeed[NUM_EVOL_GFS],
+                                        const REAL custom_f_infinity[NUM_EVOL_GFS], REAL *NRPYELL_RESTRICT gfs,
+                                        REAL *NRPYELL_RESTRICT rhs_gfs);
+
+/* Replaces apply_bcs_inner_only.c:11-27. */
+void apply_bcs_inner_only(const paramstruct *NRPYELL_RESTRICT params, const bc_struct *NRPYELL_RESTRICT bcstruct, REAL *NRPYELL_RESTRICT gfs);
+
+/* Replaces apply_bcs_outerextrap_and_inner.c:15-75 (quadratic extrapolation). */
+void apply_bcs_outerextrap_and_inner(const paramstruct *NRPYELL_RESTRICT params, const bc_struct *NRPYELL_RESTRICT bcstruct, REAL *NRPYELL_RESTRICT gfs);
+
+/* Replaces residual_all_points.c:7-112 (bitwise reference operation order). */
+void residual_all_points(const paramstruct *NRPYELL_RESTRICT params, const rfm_struct *NRPYELL_RESTRICT rfmstruct,
+                         const REAL *NRPYELL_RESTRICT auxevol_gfs, const REAL *NRPYELL_RESTRICT in_gfs,
+                         REAL *NRPYELL_RESTRICT residual_gf);
+
+/* Replaces L2_norm_of_gf.c:6-43: log10(1e-16 + sqrt(sum g^2 dV / sum dV)) over
+ * interior points with r < integration_radius.  Deterministic two-pass FP64
+ * reduction (the result does not depend on thread counts). */
+REAL L2_norm_of_gf(const paramstruct *NRPYELL_RESTRICT params, const int gf_index, const REAL integration_radius,
+                   REAL *NRPYELL_RESTRICT xx[3], const REAL *NRPYELL_RESTRICT in_gf);
+
+/* ---------------- Part 2: library extensions ---------------- */
+
+/* Status and error policy. */
+int nrpyell_last_status(void);          /* 0 = ok */
+const char *nrpyell_last_error(void);
+void nrpyell_clear_status(void);
+void nrpyell_set_exit_on_error(int enable);
+/* Layout self-description for binding checks: writes up to n ints
+ * {sizeof(paramstruct), sizeof(rfm_struct), sizeof(innerpt_bc_struct),
+ *  sizeof(outerpt_bc_struct), sizeof(bc_info_struct), sizeof(bc_struct),
+ *  sizeof(MoL_gridfunctions_struct), sizeof(griddata_struct),
+ *  offsetof(paramstruct,Nxx0), offsetof(paramstruct,outer_bc_type),
+ *  offsetof(griddata_struct,xx), offsetof(griddata_struct,bcstruct),
+ *  offsetof(griddata_struct,rfmstruct), offsetof(griddata_struct,gridfuncs),
+ *  NGHOSTS}; returns how many it wrote. */
+int nrpyell_abi_layout(int *out, int n);
+/* Number of kernel launches issued by this process so far. */
+long long nrpyell_launch_count(void);
+
+/* How MoL_step_forward_in_time runs.
+ *  NRPYELL_STEP_FUSED (default): per RK4 substep one fused RHS + update
+ *    kernel over the interior, a radiation-BC column kernel for the outer
+ *    face and an inner-ghost copy.  Inner ghost zones of y_n are treated as
+ *    images of their source points (what apply_bcs_inner_only enforces).
+ *  NRPYELL_STEP_REFERENCE_ORDER: rhs_eval, BCs and the all-points update in
+ *    the reference's order and arithmetic, for arbitrary ghost contents. */
+#define NRPYELL_STEP_FUSED 0
+#define NRPYELL_STEP_REFERENCE_ORDER 1
+void nrpyell_set_step_mode(int mode);
+int nrpyell_get_step_mode(void);
+
+/* Selects the CUDA device used by every later call (default: device 0).
+ * Call before any other GPU work in the process. */
+int nrpyell_set_device(int device);
+/* Waits for all queued GPU work of the library. */
+void nrpyell_synchronize(void);
+/* Drops every cached device table (rfm, BC maps, L2 weights, scratch). */
+void nrpyell_release_tables(void);
+
+/* Device / pinned memory for callers that keep gridfunctions resident. */
+void *nrpyell_device_malloc(size_t bytes);
+void nrpyell_device_free(void *ptr);
+void *nrpyell_host_pinned_malloc(size_t bytes);
+void nrpyell_host_pinned_free(void *ptr);
+/* kind: 0 host->device, 1 device->host, 2 device->device, 3 default. */
+int nrpyell_memcpy(void *dst, const void *src, size_t bytes, int kind);
+int nrpyell_memset(void *dst, int value, size_t bytes);
+
+/* Set-up, restated from the reference's generated set-up code (host). */
+void nrpyell_set_Cparameters_to_default(paramstruct *params);                 /* set_Cparameters_to_default.c:5-86 */
+void nrpyell_set_Nxx_dxx_invdx_params__and__xx(const int EigenCoord, const int Nxx[3], paramstruct *params,
+                                               REAL *xx[3]);                  /* set_Nxx_dxx_invdx_params__and__xx.c:5-54 */
+void nrpyell_free_xx(REAL *xx[3]);
+void nrpyell_bcstruct_set_up(const paramstruct *params, bc_struct *bcstruct);   /* bcstruct_set_up.c:350-521 */
+void nrpyell_bcstruct_free(bc_struct *bcstruct);
+void nrpyell_rfm_precompute_rfmstruct_malloc(const paramstruct *params, rfm_struct *rfmstruct);
+void nrpyell_rfm_precompute_rfmstruct_define(const paramstruct *params, REAL *xx[3], rfm_struct *rfmstruct); /* rfm_precompute_rfmstruct_define.c */
+void nrpyell_rfm_precompute_rfmstruct_freemem(const paramstruct *params, rfm_struct *rfmstruct);
+REAL nrpyell_find_timestep(const paramstruct *params, REAL *xx[3], const REAL CFL_FACTOR);               /* find_timestep.c:5-46 */
+void nrpyell_auxevol_gfs_all_points(const paramstruct *params, REAL *xx[3], REAL *auxevol_gfs);         /* auxevol_gfs_all_points.c */
+void nrpyell_wavespeed_gf_all_points(const paramstruct *params, const REAL CFL_FACTOR, const REAL dt, REAL *xx[3],
+                                     REAL *auxevol_gfs);                                                /* wavespeed_gf_all_points.c */
+REAL nrpyell_compute_wavespeed_at_OB(const paramstruct *params, const REAL *auxevol_gfs);               /* compute_wavespeed_at_OB.c */
+
+/* Stop-on-tolerance relaxation on device-resident gridfunctions.
+ * For n = 0, 1, ..., max_steps: evaluate the residual of y_n and its L2 norm
+ * (integration_radius as in L2_norm_of_gf); stop when log10 L2 <= log10_tol,
+ * otherwise take one RK4 step (main.c:138-187 order, plus the stop test of the
+ * Einstein Toolkit driver).  griddata->params must already carry the
+ * wavespeeds at the outer boundary.  history (nullable) receives log10 L2 of
+ * every evaluated n (max_steps+1 entries).  Returns 0 when converged, 1 when
+ * max_steps was reached, negative on error. */
+int nrpyell_relax(griddata_struct *griddata, const REAL dt, const REAL log10_tol, const int max_steps,
+                  const REAL integration_radius, int *steps_taken, REAL *final_log10_l2, REAL *history);
+
+/* The same solve with host buffers: copies auxevol_host (3 gfs) and
+ * y_n_host (2 gfs, the initial guess) to the device, relaxes, copies the
+ * solution back into y_n_host. */
+int nrpyell_relax_host(const paramstruct *params, REAL *xx[3], const bc_struct *bcstruct, const rfm_struct *rfmstruct,
+                       const REAL *auxevol_host, REAL *y_n_host, const REAL dt, const REAL log10_tol, const int max_steps,
+                       const REAL integration_radius, int *steps_taken, REAL *final_log10_l2);
+
+/* Timing on the library's stream.  nrpyell_event_record(slot) records CUDA
+ * event `slot` (0..15); nrpyell_event_elapsed_ms(a, b) waits for event b and
+ * returns the device time from a to b in milliseconds. */
+int nrpyell_event_record(int slot);
+float nrpyell_event_elapsed_ms(int a, int b);
+/* Writes a 256 MiB device buffer, evicting the 126 MB L2 (benchmark hygiene). */
+void nrpyell_flush_l2(void);
+/* Device time of the fused RK4 pieces on griddata's buffers, averaged over
+ * n_iter launches replayed from a CUDA graph (the buffers are modified):
+ *   ms_interior: one fused interior kernel of RK4 stage `stage` (1..4)
+ *   ms_step:     one whole RK4 step (4 stages x interior/outer-BC/ghost kernels) */
+int nrpyell_time_fused(griddata_struct *griddata, const REAL dt, const int stage, const int n_iter, double *ms_interior,
+                       double *ms_step);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* NRPYELL_GPU_H */

@@ -1,0 +1,63 @@
+// Shared definitions for the CUDA sources of libnrpyell_gpu.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+#include <stdio.h>
+
+#include "nrpyell_gpu.h"
+
+namespace nrpyell {
+
+// Error handling: record the first failure, optionally exit(1) like the
+// reference does on set-up errors.
+void report_error(const char* file, int line, const char* what);
+bool status_ok();
+cudaStream_t stream();
+void count_launch(int n = 1);
+
+#define NRPYELL_CUDA(call)                                                     \
+  do {                                                                         \
+    cudaError_t e_ = (call);                                                   \
+    if (e_ != cudaSuccess) {                                                   \
+      char b_[512];                                                            \
+      snprintf(b_, sizeof(b_), "%s: %s", #call, cudaGetErrorString(e_));       \
+      ::nrpyell::report_error(__FILE__, __LINE__, b_);                         \
+    }                                                                          \
+  } while (0)
+
+#define NRPYELL_FAIL(msg) ::nrpyell::report_error(__FILE__, __LINE__, (msg))
+
+// Launch bookkeeping: every kernel launch of the library goes through this,
+// so the process can report how many of its own kernels ran.
+#define NRPYELL_LAUNCH(kernel, grid, block, smem, ...)                         \
+  do {                                                                         \
+    kernel<<<(grid), (block), (smem), ::nrpyell::stream()>>>(__VA_ARGS__);     \
+    ::nrpyell::count_launch();                                                 \
+    NRPYELL_CUDA(cudaGetLastError());                                          \
+  } while (0)
+
+// Grid geometry passed by value to kernels.
+struct Dims {
+  int N0, N1, N2;        // Nxx_plus_2NGHOSTS{0,1,2}
+  int Nxx0, Nxx1, Nxx2;  // interior sizes
+  long long Ntot;        // N0*N1*N2
+};
+
+inline Dims dims_of(const paramstruct* p) {
+  Dims d;
+  d.N0 = p->Nxx_plus_2NGHOSTS0;
+  d.N1 = p->Nxx_plus_2NGHOSTS1;
+  d.N2 = p->Nxx_plus_2NGHOSTS2;
+  d.Nxx0 = p->Nxx0;
+  d.Nxx1 = p->Nxx1;
+  d.Nxx2 = p->Nxx2;
+  d.Ntot = (long long)d.N0 * d.N1 * d.N2;
+  return d;
+}
+
+// Checks that ptr can be dereferenced by the GPU (device, managed or mapped
+// host memory).  Returns false and records an error otherwise.
+bool check_device_pointer(const void* ptr, const char* what);
+
+}  // namespace nrpyell

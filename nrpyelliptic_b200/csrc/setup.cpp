@@ -1,0 +1,384 @@
+// Host-side set-up: parameters, grid, reference-metric tables, puncture
+// source terms, wavespeed, time step and boundary-condition maps.
+//
+// These restate the reference's generated set-up functions (cited per
+// function) so the library can build every hot-path input on its own, e.g.
+// on a machine without the reference sources or for batches of puncture
+// configurations.  Formulas keep the reference's algebraic form so that the
+// tables agree with the reference's to rounding.
+#include <math.h>
+#include <stdio.h>
+#include <stdlib.h>
+#include <string.h>
+
+#include "nrpyell_gpu.h"
+#include "sinhsymtp.h"
+
+extern "C" {
+
+// set_Cparameters_to_default.c:5-86
+void nrpyell_set_Cparameters_to_default(paramstruct *p) {
+  memset(p, 0, sizeof(*p));
+  p->Nxx0 = 64; p->Nxx1 = 32; p->Nxx2 = 64;
+  p->Nxx_plus_2NGHOSTS0 = 70; p->Nxx_plus_2NGHOSTS1 = 38; p->Nxx_plus_2NGHOSTS2 = 70;
+  p->xx0 = p->xx1 = p->xx2 = 1e300;
+  p->dxx0 = p->dxx1 = p->dxx2 = 0.1;
+  p->xxmin0 = p->xxmin1 = p->xxmin2 = 0.1;
+  p->xxmax0 = p->xxmax1 = p->xxmax2 = 0.1;
+  p->invdx0 = p->invdx1 = p->invdx2 = 1.0;
+  p->Cart_originx = p->Cart_originy = p->Cart_originz = 0.0;
+  p->Cart_CoM_offsetx = p->Cart_CoM_offsety = p->Cart_CoM_offsetz = 0.0;
+  REAL *rfm_params[] = {&p->f0_of_xx0, &p->f1_of_xx1, &p->f2_of_xx1, &p->f2_of_xx0_xx1, &p->f3_of_xx0,
+                        &p->f4_of_xx2, &p->f0_of_xx0__D0, &p->f0_of_xx0__DD00, &p->f0_of_xx0__DDD000,
+                        &p->f1_of_xx1__D1, &p->f1_of_xx1__DD11, &p->f1_of_xx1__DDD111, &p->f2_of_xx1__D1,
+                        &p->f2_of_xx1__DD11, &p->f2_of_xx1__DDD111, &p->f2_of_xx0_xx1__D0, &p->f2_of_xx0_xx1__D1,
+                        &p->f2_of_xx0_xx1__DD00, &p->f2_of_xx0_xx1__DD11, &p->f3_of_xx0__D0, &p->f3_of_xx0__DD00,
+                        &p->f4_of_xx2__D2, &p->f4_of_xx2__DD22};
+  for (size_t i = 0; i < sizeof(rfm_params) / sizeof(rfm_params[0]); i++) *rfm_params[i] = 1e300;
+  p->bScale = 0.5;
+  p->SINHWAA = 0.2;
+  p->AMAX = 10.0;
+  p->eta_damping = 1.0;
+  p->time = 0.0;
+  p->uu_wavespeed_at_OB = 1.0;
+  p->vv_wavespeed_at_OB = 1.0;
+  p->bare_mass_0 = 1.0;
+  p->bare_mass_1 = 0.0;
+  p->S0_z = 0.2;
+  p->has_outer_boundary = 0;
+  p->outer_bc_type = EXTRAPOLATION_OUTER_BCS;
+}
+
+// set_Nxx_dxx_invdx_params__and__xx.c:5-54.  Cell-centred uniform grid,
+// xx[j] = xxmin + (j - NGHOSTS + 1/2) dxx.  EigenCoord=1 is SymTP with xx0 in
+// (0, AMAX); EigenCoord=0 is SinhSymTP with xx0 in (0, 1).
+void nrpyell_set_Nxx_dxx_invdx_params__and__xx(const int EigenCoord, const int Nxx[3], paramstruct *p, REAL *xx[3]) {
+  p->Nxx0 = Nxx[0]; p->Nxx1 = Nxx[1]; p->Nxx2 = Nxx[2];
+  p->Nxx_plus_2NGHOSTS0 = Nxx[0] + 2 * NGHOSTS;
+  p->Nxx_plus_2NGHOSTS1 = Nxx[1] + 2 * NGHOSTS;
+  p->Nxx_plus_2NGHOSTS2 = Nxx[2] + 2 * NGHOSTS;
+  const REAL xxmin[3] = {0.0, 0.0, -M_PI};
+  const REAL xxmax[3] = {EigenCoord == 0 ? 1.0 : p->AMAX, M_PI, M_PI};
+  REAL *dxx[3] = {&p->dxx0, &p->dxx1, &p->dxx2};
+  REAL *invdx[3] = {&p->invdx0, &p->invdx1, &p->invdx2};
+  const int Ng[3] = {p->Nxx_plus_2NGHOSTS0, p->Nxx_plus_2NGHOSTS1, p->Nxx_plus_2NGHOSTS2};
+  for (int d = 0; d < 3; d++) {
+    *dxx[d] = (xxmax[d] - xxmin[d]) / ((REAL)Nxx[d]);
+    *invdx[d] = 1.0 / *dxx[d];
+    xx[d] = (REAL *)malloc(sizeof(REAL) * Ng[d]);
+    // one rounding, as the reference's FMA-contracted build computes it
+    for (int j = 0; j < Ng[d]; j++) xx[d][j] = fma(((REAL)(j - NGHOSTS) + (1.0 / 2.0)), *dxx[d], xxmin[d]);
+  }
+}
+
+void nrpyell_free_xx(REAL *xx[3]) {
+  for (int d = 0; d < 3; d++) {
+    free(xx[d]);
+    xx[d] = NULL;
+  }
+}
+
+// rfm_precompute_rfmstruct_malloc.c / _freemem.c
+void nrpyell_rfm_precompute_rfmstruct_malloc(const paramstruct *p, rfm_struct *r) {
+  const size_t n0 = p->Nxx_plus_2NGHOSTS0, n1 = p->Nxx_plus_2NGHOSTS1;
+  r->f0_of_xx0 = (REAL *)malloc(sizeof(REAL) * n0);
+  r->f0_of_xx0__D0 = (REAL *)malloc(sizeof(REAL) * n0);
+  r->f0_of_xx0__DD00 = (REAL *)malloc(sizeof(REAL) * n0);
+  r->f0_of_xx0__DDD000 = (REAL *)malloc(sizeof(REAL) * n0);
+  r->f1_of_xx1 = (REAL *)malloc(sizeof(REAL) * n1);
+  r->f1_of_xx1__D1 = (REAL *)malloc(sizeof(REAL) * n1);
+  r->f1_of_xx1__DD11 = (REAL *)malloc(sizeof(REAL) * n1);
+  r->f2_of_xx0_xx1 = (REAL *)malloc(sizeof(REAL) * n0 * n1);
+  r->f2_of_xx0_xx1__D0 = (REAL *)malloc(sizeof(REAL) * n0 * n1);
+  r->f2_of_xx0_xx1__D1 = (REAL *)malloc(sizeof(REAL) * n0 * n1);
+  r->f2_of_xx0_xx1__DD00 = (REAL *)malloc(sizeof(REAL) * n0 * n1);
+  r->f2_of_xx0_xx1__DD11 = (REAL *)malloc(sizeof(REAL) * n0 * n1);
+  r->f3_of_xx0 = (REAL *)malloc(sizeof(REAL) * n0);
+  r->f3_of_xx0__D0 = (REAL *)malloc(sizeof(REAL) * n0);
+  r->f3_of_xx0__DD00 = (REAL *)malloc(sizeof(REAL) * n0);
+}
+
+void nrpyell_rfm_precompute_rfmstruct_freemem(const paramstruct *p, rfm_struct *r) {
+  (void)p;
+  REAL *NRPYELL_RESTRICT *a[] = {&r->f0_of_xx0, &r->f0_of_xx0__D0, &r->f0_of_xx0__DD00, &r->f0_of_xx0__DDD000, &r->f1_of_xx1,
+                &r->f1_of_xx1__D1, &r->f1_of_xx1__DD11, &r->f2_of_xx0_xx1, &r->f2_of_xx0_xx1__D0,
+                &r->f2_of_xx0_xx1__D1, &r->f2_of_xx0_xx1__DD00, &r->f2_of_xx0_xx1__DD11, &r->f3_of_xx0,
+                &r->f3_of_xx0__D0, &r->f3_of_xx0__DD00};
+  for (size_t i = 0; i < sizeof(a) / sizeof(a[0]); i++) {
+    free(*a[i]);
+    *a[i] = NULL;
+  }
+}
+
+// rfm_precompute_rfmstruct_define.c:5-93.  With E(x) = exp(x/w) - exp(-x/w),
+// C(x) = exp(x/w) + exp(-x/w), D = exp(1/w) - exp(-1/w) and A = AMAX E/D:
+//   f0 = A, f0' = AMAX C/(w D), f0'' = AMAX E/(w^2 D), f0''' = AMAX C/(w^3 D)
+//   f1 = sin xx1, f1' = cos xx1, f1'' = -sin xx1
+//   f2 = sqrt(A^2 + b^2 sin^2 xx1) and its xx0/xx1 derivatives
+//   f3 = sqrt(A^2 + b^2) and its xx0 derivatives.
+void nrpyell_rfm_precompute_rfmstruct_define(const paramstruct *p, REAL *xx[3], rfm_struct *r) {
+  const REAL AMAX = p->AMAX, SINHWAA = p->SINHWAA, bScale = p->bScale;
+  const int N0 = p->Nxx_plus_2NGHOSTS0, N1 = p->Nxx_plus_2NGHOSTS1;
+  const REAL D = exp(1.0 / SINHWAA) - exp(-1 / SINHWAA);
+  for (int i0 = 0; i0 < N0; i0++) {
+    const REAL x = xx[0][i0];
+    const REAL ep = exp(x / SINHWAA), em = exp(-x / SINHWAA);
+    r->f0_of_xx0[i0] = AMAX * (ep - em) / D;
+    r->f0_of_xx0__D0[i0] = AMAX * (ep / SINHWAA + em / SINHWAA) / D;
+    r->f0_of_xx0__DD00[i0] = AMAX * (ep / pow(SINHWAA, 2) - em / pow(SINHWAA, 2)) / D;
+    r->f0_of_xx0__DDD000[i0] = AMAX * (ep / pow(SINHWAA, 3) + em / pow(SINHWAA, 3)) / D;
+    const REAL A2 = pow(AMAX, 2) * pow(ep - em, 2) / pow(D, 2);
+    const REAL f3 = sqrt(A2 + pow(bScale, 2));
+    const REAL dA2 = (1.0 / 2.0) * pow(AMAX, 2) * (2 * ep / SINHWAA + 2 * em / SINHWAA) * (ep - em);  // (A^2)'/2 * D^2
+    r->f3_of_xx0[i0] = f3;
+    r->f3_of_xx0__D0[i0] = dA2 / (f3 * pow(D, 2));
+    r->f3_of_xx0__DD00[i0] =
+        -1.0 / 4.0 * pow(AMAX, 4) * pow(2 * ep / SINHWAA + 2 * em / SINHWAA, 2) * pow(ep - em, 2) /
+            (pow(A2 + pow(bScale, 2), 3.0 / 2.0) * pow(D, 4)) +
+        (1.0 / 2.0) * pow(AMAX, 2) * (2 * ep / pow(SINHWAA, 2) - 2 * em / pow(SINHWAA, 2)) * (ep - em) / (f3 * pow(D, 2)) +
+        (1.0 / 2.0) * pow(AMAX, 2) * (ep / SINHWAA + em / SINHWAA) * (2 * ep / SINHWAA + 2 * em / SINHWAA) / (f3 * pow(D, 2));
+  }
+  for (int i1 = 0; i1 < N1; i1++) {
+    const REAL y = xx[1][i1];
+    r->f1_of_xx1[i1] = sin(y);
+    r->f1_of_xx1__D1[i1] = cos(y);
+    r->f1_of_xx1__DD11[i1] = -sin(y);
+  }
+  for (int i1 = 0; i1 < N1; i1++) {
+    const REAL y = xx[1][i1];
+    const REAL s = sin(y), c = cos(y);
+    for (int i0 = 0; i0 < N0; i0++) {
+      const REAL x = xx[0][i0];
+      const REAL ep = exp(x / SINHWAA), em = exp(-x / SINHWAA);
+      const REAL A2 = pow(AMAX, 2) * pow(ep - em, 2) / pow(D, 2);
+      const REAL q = A2 + pow(bScale, 2) * pow(s, 2);
+      const REAL f2 = sqrt(q);
+      const int k = i0 + N0 * i1;
+      r->f2_of_xx0_xx1[k] = f2;
+      r->f2_of_xx0_xx1__D0[k] =
+          (1.0 / 2.0) * pow(AMAX, 2) * (2 * ep / SINHWAA + 2 * em / SINHWAA) * (ep - em) / (f2 * pow(D, 2));
+      r->f2_of_xx0_xx1__D1[k] = pow(bScale, 2) * s * c / f2;
+      r->f2_of_xx0_xx1__DD00[k] =
+          -1.0 / 4.0 * pow(AMAX, 4) * pow(2 * ep / SINHWAA + 2 * em / SINHWAA, 2) * pow(ep - em, 2) /
+              (pow(q, 3.0 / 2.0) * pow(D, 4)) +
+          (1.0 / 2.0) * pow(AMAX, 2) * (2 * ep / pow(SINHWAA, 2) - 2 * em / pow(SINHWAA, 2)) * (ep - em) / (f2 * pow(D, 2)) +
+          (1.0 / 2.0) * pow(AMAX, 2) * (ep / SINHWAA + em / SINHWAA) * (2 * ep / SINHWAA + 2 * em / SINHWAA) / (f2 * pow(D, 2));
+      r->f2_of_xx0_xx1__DD11[k] = -pow(bScale, 4) * pow(s, 2) * pow(c, 2) / pow(q, 3.0 / 2.0) -
+                                   pow(bScale, 2) * pow(s, 2) / f2 + pow(bScale, 2) * pow(c, 2) / f2;
+    }
+  }
+}
+
+// find_timestep.c:5-46.  The reference returns the smallest proper grid
+// spacing itself (its "CFL" factor enters only through the wavespeed
+// gridfunction), so CFL_FACTOR is accepted and not used here either.
+REAL nrpyell_find_timestep(const paramstruct *p, REAL *xx[3], const REAL CFL_FACTOR) {
+  (void)CFL_FACTOR;
+  REAL dsmin = 1e38;
+  for (int i1 = NGHOSTS; i1 < NGHOSTS + p->Nxx1; i1++)
+    for (int i0 = NGHOSTS; i0 < NGHOSTS + p->Nxx0; i0++) {
+      REAL ds[3];
+      symtp_ds(p->AMAX, p->SINHWAA, p->bScale, p->dxx0, p->dxx1, p->dxx2, xx[0][i0], xx[1][i1], ds);
+      const REAL m = fmin(fabs(ds[0]), fmin(fabs(ds[1]), fabs(ds[2])));
+      if (m < dsmin) dsmin = m;
+    }
+  return dsmin;
+}
+
+// auxevol_gfs_all_points.c:6-100: psi_background (Brill-Lindquist) and
+// ADD_times_AUU (Bowen-York A_ij A^ij) at every point, ghosts included.
+void nrpyell_auxevol_gfs_all_points(const paramstruct *p, REAL *xx[3], REAL *aux) {
+  const int N0 = p->Nxx_plus_2NGHOSTS0, N1 = p->Nxx_plus_2NGHOSTS1, N2 = p->Nxx_plus_2NGHOSTS2;
+  const size_t Ntot = (size_t)N0 * N1 * N2;
+  const ByPuncture b0 = {{p->puncture_0_x, p->puncture_0_y, p->puncture_0_z}, {p->P0_x, p->P0_y, p->P0_z},
+                         {p->S0_x, p->S0_y, p->S0_z}};
+  const ByPuncture b1 = {{p->puncture_1_x, p->puncture_1_y, p->puncture_1_z}, {p->P1_x, p->P1_y, p->P1_z},
+                         {p->S1_x, p->S1_y, p->S1_z}};
+#pragma omp parallel for
+  for (int i2 = 0; i2 < N2; i2++)
+    for (int i1 = 0; i1 < N1; i1++)
+      for (int i0 = 0; i0 < N0; i0++) {
+        double X[3];
+        symtp_xx_to_cart(p->AMAX, p->SINHWAA, p->bScale, xx[0][i0], xx[1][i1], xx[2][i2], X);
+        const size_t idx = (size_t)i0 + (size_t)N0 * ((size_t)i1 + (size_t)N1 * i2);
+        aux[PSI_BACKGROUNDGF * Ntot + idx] = bl_psi(p->bare_mass_0, b0.pos, p->bare_mass_1, b1.pos, X);
+        aux[ADD_TIMES_AUUGF * Ntot + idx] = by_AA(b0, b1, X);
+      }
+}
+
+// wavespeed_gf_all_points.c:6-45: c = CFL * min(ds) / dt on the interior.
+// The reference leaves ghost-zone wavespeeds unset; they are never read, and
+// here they are set to zero so the array is deterministic.
+void nrpyell_wavespeed_gf_all_points(const paramstruct *p, const REAL CFL_FACTOR, const REAL dt, REAL *xx[3], REAL *aux) {
+  const int N0 = p->Nxx_plus_2NGHOSTS0, N1 = p->Nxx_plus_2NGHOSTS1, N2 = p->Nxx_plus_2NGHOSTS2;
+  const size_t Ntot = (size_t)N0 * N1 * N2;
+  REAL *ws = aux + WAVESPEEDGF * Ntot;
+  memset(ws, 0, sizeof(REAL) * Ntot);
+#pragma omp parallel for
+  for (int i2 = NGHOSTS; i2 < NGHOSTS + p->Nxx2; i2++)
+    for (int i1 = NGHOSTS; i1 < NGHOSTS + p->Nxx1; i1++)
+      for (int i0 = NGHOSTS; i0 < NGHOSTS + p->Nxx0; i0++) {
+        REAL ds[3];
+        symtp_ds(p->AMAX, p->SINHWAA, p->bScale, p->dxx0, p->dxx1, p->dxx2, xx[0][i0], xx[1][i1], ds);
+        const REAL dsmin = fmin(ds[0], fmin(ds[1], ds[2]));
+        ws[(size_t)i0 + (size_t)N0 * ((size_t)i1 + (size_t)N1 * i2)] = CFL_FACTOR * dsmin / dt;
+      }
+}
+
+// compute_wavespeed_at_OB.c:6-12
+REAL nrpyell_compute_wavespeed_at_OB(const paramstruct *p, const REAL *aux) {
+  const int N0 = p->Nxx_plus_2NGHOSTS0, N1 = p->Nxx_plus_2NGHOSTS1, N2 = p->Nxx_plus_2NGHOSTS2;
+  const size_t Ntot = (size_t)N0 * N1 * N2;
+  const size_t idx = (size_t)(N0 - NGHOSTS - 1) + (size_t)N0 * ((size_t)NGHOSTS + (size_t)N1 * (N2 / 2));
+  return aux[WAVESPEEDGF * Ntot + idx];
+}
+
+// Boundary maps (bcstruct_set_up.c:350-521).  The reference classifies each
+// ghost point by mapping it to Cartesian coordinates with the SymTP
+// eigen-coordinate and back: points that map onto themselves are pure outer
+// points, all others copy from the interior (or pure outer) point they map
+// to.  For SymTP on a cell-centred grid that round trip reduces to three
+// reflections, applied here directly on the indices:
+//   xx0 < 0          -> xx0' = -xx0, xx2' = xx2 + pi   (A -> -A flips x and y)
+//   xx1 < 0 or > pi  -> xx1' = -xx1 or 2pi - xx1, xx2' = xx2 + pi
+//   xx2 outside [-pi, pi) -> wrap by 2pi.
+// i.e. i0' = 2 NG - 1 - i0 for i0 < NG (no reflection at the outer xx0 face),
+// i1' = 2 NG - 1 - i1 or 2 (NG + Nxx1) - 1 - i1, i2' = wrap(i2 + Nxx2/2).
+// The test suite checks the result against the reference's own bcstruct.
+// The parity signs (only parity[0], +1, is used by the scalar gridfunctions
+// uu and vv) are the signs of the unit-vector dot products e_i . e_i'.
+static void symtp_unit_dots(const paramstruct *p, REAL x0, REAL x1, REAL x2, REAL y0, REAL y1, REAL y2, REAL d[3]) {
+  const REAL A = symtp_A_invw(p->AMAX, p->SINHWAA, x0), Ap = symtp_A_invw(p->AMAX, p->SINHWAA, y0);
+  const REAL b2 = p->bScale * p->bScale;
+  const REAL B = sqrt(A * A + b2), Bp = sqrt(Ap * Ap + b2);
+  const REAL n = sqrt(A * A + b2 * sin(x1) * sin(x1)), np = sqrt(Ap * Ap + b2 * sin(y1) * sin(y1));
+  const REAL cphi = cos(x2) * cos(y2) + sin(x2) * sin(y2);
+  // e0 ~ (B sin cos, B sin sin, A cos)/n ;  e1 ~ (A cos cos, A cos sin, -B sin)/n ; e2 ~ (-sin, cos, 0)
+  d[0] = (B * Bp * sin(x1) * sin(y1) * cphi + A * Ap * cos(x1) * cos(y1)) / (n * np);
+  d[1] = (A * Ap * cos(x1) * cos(y1) * cphi + B * Bp * sin(x1) * sin(y1)) / (n * np);
+  d[2] = cphi;
+}
+
+void nrpyell_bcstruct_set_up(const paramstruct *p, bc_struct *bc) {
+  const int N0 = p->Nxx_plus_2NGHOSTS0, N1 = p->Nxx_plus_2NGHOSTS1, N2 = p->Nxx_plus_2NGHOSTS2;
+  const int Nxx1 = p->Nxx1, Nxx2 = p->Nxx2;
+  memset(bc, 0, sizeof(*bc));
+  // Final SinhSymTP coordinates (for the parity dot products only).
+  REAL *xx[3];
+  paramstruct q = *p;
+  const int Nxx[3] = {p->Nxx0, p->Nxx1, p->Nxx2};
+  nrpyell_set_Nxx_dxx_invdx_params__and__xx(0, Nxx, &q, xx);
+
+  auto map_point = [&](int i0, int i1, int i2, int out[3]) {
+    int shift = 0;
+    if (i0 < NGHOSTS) {
+      i0 = 2 * NGHOSTS - 1 - i0;
+      shift ^= 1;
+    }
+    if (i1 < NGHOSTS) {
+      i1 = 2 * NGHOSTS - 1 - i1;
+      shift ^= 1;
+    } else if (i1 >= NGHOSTS + Nxx1) {
+      i1 = 2 * (NGHOSTS + Nxx1) - 1 - i1;
+      shift ^= 1;
+    }
+    int j = i2 - NGHOSTS;  // interior index in [0, Nxx2) after wrapping
+    if (shift) j += Nxx2 / 2;
+    j %= Nxx2;
+    if (j < 0) j += Nxx2;
+    out[0] = i0;
+    out[1] = i1;
+    out[2] = j + NGHOSTS;
+  };
+  auto interior = [&](int i0, int i1, int i2) {
+    return i0 >= NGHOSTS && i0 < N0 - NGHOSTS && i1 >= NGHOSTS && i1 < N1 - NGHOSTS && i2 >= NGHOSTS &&
+           i2 < N2 - NGHOSTS;
+  };
+
+  // Step 1: inner points, in the reference's loop order (i2 outer, i0 inner).
+  int num_inner = 0;
+  for (int i2 = 0; i2 < N2; i2++)
+    for (int i1 = 0; i1 < N1; i1++)
+      for (int i0 = 0; i0 < N0; i0++) {
+        if (interior(i0, i1, i2)) continue;
+        int m[3];
+        map_point(i0, i1, i2, m);
+        if (!(m[0] == i0 && m[1] == i1 && m[2] == i2)) num_inner++;
+      }
+  bc->bc_info.num_inner_boundary_points = num_inner;
+  bc->inner_bc_array = (innerpt_bc_struct *)malloc(sizeof(innerpt_bc_struct) * (num_inner > 0 ? num_inner : 1));
+  int w = 0;
+  for (int i2 = 0; i2 < N2; i2++)
+    for (int i1 = 0; i1 < N1; i1++)
+      for (int i0 = 0; i0 < N0; i0++) {
+        if (interior(i0, i1, i2)) continue;
+        int m[3];
+        map_point(i0, i1, i2, m);
+        if (m[0] == i0 && m[1] == i1 && m[2] == i2) continue;
+        innerpt_bc_struct &e = bc->inner_bc_array[w++];
+        e.dstpt = i0 + N0 * (i1 + N1 * i2);
+        e.srcpt = m[0] + N0 * (m[1] + N1 * m[2]);
+        REAL d[3];
+        symtp_unit_dots(&q, xx[0][i0], xx[1][i1], xx[2][i2], xx[0][m[0]], xx[1][m[1]], xx[2][m[2]], d);
+        const REAL par[10] = {1, d[0], d[1], d[2], d[0] * d[0], d[0] * d[1], d[0] * d[2], d[1] * d[1], d[1] * d[2], d[2] * d[2]};
+        for (int t = 0; t < 10; t++) e.parity[t] = (par[t] < 0) ? -1 : 1;
+      }
+
+  // Step 2: pure outer points, grown layer by layer: x0 faces, then x1, then x2
+  // (bcstruct_set_up.c:404-518).
+  int imin[3] = {NGHOSTS, NGHOSTS, NGHOSTS};
+  int imax[3] = {N0 - NGHOSTS, N1 - NGHOSTS, N2 - NGHOSTS};
+  for (int gz = 0; gz < NGHOSTS; gz++) {
+    int r[6][6];
+    const int x0min[6] = {imin[0] - 1, imin[0], imin[1], imax[1], imin[2], imax[2]}; imin[0]--;
+    const int x0max[6] = {imax[0], imax[0] + 1, imin[1], imax[1], imin[2], imax[2]}; imax[0]++;
+    const int x1min[6] = {imin[0], imax[0], imin[1] - 1, imin[1], imin[2], imax[2]}; imin[1]--;
+    const int x1max[6] = {imin[0], imax[0], imax[1], imax[1] + 1, imin[2], imax[2]}; imax[1]++;
+    const int x2min[6] = {imin[0], imax[0], imin[1], imax[1], imin[2] - 1, imin[2]}; imin[2]--;
+    const int x2max[6] = {imin[0], imax[0], imin[1], imax[1], imax[2], imax[2] + 1}; imax[2]++;
+    const int *faces[6] = {x0min, x0max, x1min, x1max, x2min, x2max};
+    for (int f = 0; f < 6; f++)
+      for (int i = 0; i < 6; i++) r[f][i] = faces[f][i], bc->bc_info.bc_loop_bounds[gz][f][i] = faces[f][i];
+    for (int dirn = 0; dirn < 3; dirn++) {
+      int count = 0;
+      for (int pass = 0; pass < 2; pass++) {
+        int idx2d = 0;
+        outerpt_bc_struct *arr = pass ? bc->pure_outer_bc_array[dirn + 3 * gz] : NULL;
+        for (int side = 0; side < 2; side++) {
+          const int face = 2 * dirn + side;
+          const int *b = r[face];
+          const int8_t F0 = (face == 0) - (face == 1), F1 = (face == 2) - (face == 3), F2 = (face == 4) - (face == 5);
+          for (int i2 = b[4]; i2 < b[5]; i2++)
+            for (int i1 = b[2]; i1 < b[3]; i1++)
+              for (int i0 = b[0]; i0 < b[1]; i0++) {
+                int m[3];
+                map_point(i0, i1, i2, m);
+                if (!(m[0] == i0 && m[1] == i1 && m[2] == i2)) continue;
+                if (arr) {
+                  arr[idx2d].i0 = (short)i0; arr[idx2d].i1 = (short)i1; arr[idx2d].i2 = (short)i2;
+                  arr[idx2d].FACEX0 = F0; arr[idx2d].FACEX1 = F1; arr[idx2d].FACEX2 = F2;
+                }
+                idx2d++;
+              }
+        }
+        if (!pass) {
+          count = idx2d;
+          bc->pure_outer_bc_array[dirn + 3 * gz] = (outerpt_bc_struct *)malloc(sizeof(outerpt_bc_struct) * (count > 0 ? count : 1));
+        }
+      }
+      bc->bc_info.num_pure_outer_boundary_points[gz][dirn] = count;
+    }
+  }
+  nrpyell_free_xx(xx);
+}
+
+void nrpyell_bcstruct_free(bc_struct *bc) {
+  free(bc->inner_bc_array);
+  bc->inner_bc_array = NULL;
+  for (int i = 0; i < NGHOSTS * 3; i++) {
+    free(bc->pure_outer_bc_array[i]);
+    bc->pure_outer_bc_array[i] = NULL;
+  }
+}
+
+}  // extern "C"
