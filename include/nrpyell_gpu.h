@@ -15,8 +15,8 @@
  * into a recorded status (nrpyell_last_status / nrpyell_last_error).
  *
  * Threading: one host thread, one CUDA stream per process; calls run in
- * program order on that stream.  L2_norm_of_gf is the only Part-1 call that
- * waits for the GPU (it returns a host scalar).
+ * program order on that stream and, by default, return when their GPU work
+ * is done (see nrpyell_set_async).
  */
 #ifndef NRPYELL_GPU_H
 #define NRPYELL_GPU_H
@@ -104,6 +104,11 @@ long long nrpyell_launch_count(void);
 void nrpyell_set_step_mode(int mode);
 int nrpyell_get_step_mode(void);
 
+/* Part-1 calls return after their GPU work has finished (default), like the
+ * reference's functions, so the host may read managed gridfunctions right
+ * away.  nrpyell_set_async(1) lets them return after enqueueing; the caller
+ * then orders host access with nrpyell_synchronize(). */
+void nrpyell_set_async(int enable);
 /* Selects the CUDA device used by every later call (default: device 0).
  * Call before any other GPU work in the process. */
 int nrpyell_set_device(int device);

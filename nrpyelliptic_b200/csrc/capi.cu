@@ -18,6 +18,7 @@ std::string g_error;
 bool g_exit_on_error = true;
 long long g_launches = 0;
 int g_step_mode = NRPYELL_STEP_FUSED;
+bool g_async = false;
 cudaStream_t g_stream = nullptr;
 }  // namespace
 
@@ -112,11 +113,14 @@ struct FusedWork {
   int history_len;
 };
 static std::vector<FusedWork*> g_work;
+static int g_work_generation = 0;  // bumped when a work buffer is reallocated
 
+// Never call while a stream is being captured (it may allocate).
 static FusedWork* get_work(const Dims& d, int history_len) {
   for (FusedWork* w : g_work)
     if (w->d.Nxx1 == d.Nxx1 && w->d.Nxx2 == d.Nxx2 && w->d.N0 == d.N0 && w->d.N1 == d.N1 && w->d.N2 == d.N2) {
       if (w->history_len < history_len) {
+        g_work_generation++;
         NRPYELL_CUDA(cudaStreamSynchronize(stream()));
         NRPYELL_CUDA(cudaFree(w->history));
         NRPYELL_CUDA(cudaMalloc(&w->history, sizeof(double) * history_len));
@@ -153,8 +157,8 @@ static bool fused_ready(griddata_struct* g, RfmTables** rt, BcTables** bt) {
   return *rt && *bt && (*bt)->columns_ok && p->outer_bc_type == RADIATION_OUTER_BCS;
 }
 
-static FusedArgs fused_args(griddata_struct* g, RfmTables* rt, BcTables* bt, FusedWork* w, double dt, int stage,
-                            const int* done) {
+static FusedArgs fused_args(griddata_struct* g, RfmTables* rt, BcTables* bt, FusedWork* w, Scratch* s, double dt,
+                            int stage, const int* done) {
   const paramstruct* p = &g->params;
   MoL_gridfunctions_struct* gf = &g->gridfuncs;
   FusedArgs a;
@@ -174,7 +178,7 @@ static FusedArgs fused_args(griddata_struct* g, RfmTables* rt, BcTables* bt, Fus
   a.bt = bt;
   a.lt = nullptr;
   a.face = w->face;
-  a.s = get_scratch(fused_interior_blocks(a.d));
+  a.s = s;
   a.done = done;
   return a;
 }
@@ -186,8 +190,10 @@ static void mol_step_fused(griddata_struct* g, double dt) {
     mol_step_reference_order(g, dt);
     return;
   }
-  FusedWork* w = get_work(dims_of(&g->params), 16);
-  for (int s = 1; s <= 4; s++) launch_fused_substep<double>(s, fused_args(g, rt, bt, w, dt, s, w->zero_flag));
+  const Dims d = dims_of(&g->params);
+  FusedWork* w = get_work(d, 16);
+  Scratch* sc = get_scratch(fused_interior_blocks(d));
+  for (int s = 1; s <= 4; s++) launch_fused_substep<double>(s, fused_args(g, rt, bt, w, sc, dt, s, w->zero_flag));
 }
 
 static bool check_gridfuncs(const MoL_gridfunctions_struct* gf) {
@@ -206,6 +212,7 @@ struct RelaxGraph {
   griddata_struct key;
   double dt, tol, R;
   int max_steps;
+  int scratch_gen, work_gen;  // buffers the graph was captured with
   cudaGraphExec_t exec;
   size_t nodes;
 };
@@ -224,6 +231,14 @@ static bool same_grid(const griddata_struct* a, const griddata_struct* b) {
          a->xx[2] == b->xx[2] && a->bcstruct.inner_bc_array == b->bcstruct.inner_bc_array &&
          a->rfmstruct.f0_of_xx0 == b->rfmstruct.f0_of_xx0 &&
          memcmp(&a->gridfuncs, &b->gridfuncs, sizeof(MoL_gridfunctions_struct)) == 0;
+}
+
+// The reference's functions return when their work is done, and callers such
+// as main.c read managed gridfunctions on the host right after a call; the
+// Part-1 entry points therefore wait for their kernels unless the caller
+// opted into asynchronous calls.
+static void finish_call() {
+  if (!g_async) NRPYELL_CUDA(cudaStreamSynchronize(stream()));
 }
 
 }  // namespace nrpyell
@@ -264,6 +279,7 @@ int nrpyell_abi_layout(int* out, int n) {
 }
 
 void nrpyell_set_step_mode(int mode) { g_step_mode = mode; }
+void nrpyell_set_async(int enable) { g_async = enable != 0; }
 int nrpyell_get_step_mode(void) { return g_step_mode; }
 
 int nrpyell_set_device(int device) {
@@ -318,6 +334,7 @@ int nrpyell_time_fused(griddata_struct* g, const REAL dt, const int stage, const
   }
   const Dims d = dims_of(&g->params);
   FusedWork* w = get_work(d, 16);
+  Scratch* sc = get_scratch(fused_interior_blocks(d));
   cudaEvent_t e0, e1;
   NRPYELL_CUDA(cudaEventCreate(&e0));
   NRPYELL_CUDA(cudaEventCreate(&e1));
@@ -328,9 +345,10 @@ int nrpyell_time_fused(griddata_struct* g, const REAL dt, const int stage, const
     NRPYELL_CUDA(cudaStreamBeginCapture(stream(), cudaStreamCaptureModeThreadLocal));
     for (int i = 0; i < n_iter; i++) {
       if (which == 0) {
-        launch_fused_interior_only<double>(stage, fused_args(g, rt, bt, w, dt, stage, w->zero_flag));
+        launch_fused_interior_only<double>(stage, fused_args(g, rt, bt, w, sc, dt, stage, w->zero_flag));
       } else {
-        for (int s = 1; s <= 4; s++) launch_fused_substep<double>(s, fused_args(g, rt, bt, w, dt, s, w->zero_flag));
+        for (int s = 1; s <= 4; s++)
+          launch_fused_substep<double>(s, fused_args(g, rt, bt, w, sc, dt, s, w->zero_flag));
       }
     }
     NRPYELL_CUDA(cudaStreamEndCapture(stream(), &graph));
@@ -439,6 +457,7 @@ void rhs_eval(const paramstruct* params, const rfm_struct* rfmstruct, const REAL
   RfmTables* rt = get_rfm_tables(params, rfmstruct);
   if (!rt) return;
   launch_rhs_ref(dims_of(params), params, rt, auxevol_gfs, in_gfs, rhs_gfs);
+  finish_call();
 }
 
 void residual_all_points(const paramstruct* params, const rfm_struct* rfmstruct, const REAL* auxevol_gfs,
@@ -449,6 +468,7 @@ void residual_all_points(const paramstruct* params, const rfm_struct* rfmstruct,
   RfmTables* rt = get_rfm_tables(params, rfmstruct);
   if (!rt) return;
   launch_residual_ref(dims_of(params), rt, auxevol_gfs, in_gfs, residual_gf);
+  finish_call();
 }
 
 void apply_bcs_outerradiation_and_inner(const paramstruct* params, const bc_struct* bcstruct,
@@ -461,6 +481,7 @@ void apply_bcs_outerradiation_and_inner(const paramstruct* params, const bc_stru
   const Dims d = dims_of(params);
   launch_radiation_bc(d, params, bt, custom_wavespeed, custom_f_infinity, gfs, rhs_gfs);
   launch_inner_copy(d, bt, rhs_gfs, NUM_EVOL_GFS);
+  finish_call();
 }
 
 void apply_bcs_inner_only(const paramstruct* params, const bc_struct* bcstruct, REAL* gfs) {
@@ -469,6 +490,7 @@ void apply_bcs_inner_only(const paramstruct* params, const bc_struct* bcstruct, 
   BcTables* bt = get_bc_tables(params, bcstruct, noxx);
   if (!bt) return;
   launch_inner_copy(dims_of(params), bt, gfs, NUM_EVOL_GFS);
+  finish_call();
 }
 
 void apply_bcs_outerextrap_and_inner(const paramstruct* params, const bc_struct* bcstruct, REAL* gfs) {
@@ -477,6 +499,7 @@ void apply_bcs_outerextrap_and_inner(const paramstruct* params, const bc_struct*
   BcTables* bt = get_bc_tables(params, bcstruct, noxx);
   if (!bt) return;
   launch_extrap_bc(dims_of(params), bt, bcstruct, gfs);
+  finish_call();
 }
 
 void MoL_step_forward_in_time(griddata_struct* griddata, const REAL dt) {
@@ -485,6 +508,7 @@ void MoL_step_forward_in_time(griddata_struct* griddata, const REAL dt) {
     mol_step_reference_order(griddata, dt);
   else
     mol_step_fused(griddata, dt);
+  finish_call();
 }
 
 REAL L2_norm_of_gf(const paramstruct* params, const int gf_index, const REAL integration_radius,
@@ -524,20 +548,31 @@ int nrpyell_relax(griddata_struct* g, const REAL dt, const REAL log10_tol, const
   Scratch* s = get_scratch(nblk);
 
   RelaxGraph* rg = nullptr;
-  for (RelaxGraph* r : g_graphs)
+  for (size_t i = 0; i < g_graphs.size(); i++) {
+    RelaxGraph* r = g_graphs[i];
+    if (r->scratch_gen != scratch_generation() || r->work_gen != g_work_generation) {
+      // captured with buffers that have since been reallocated
+      NRPYELL_CUDA(cudaGraphExecDestroy(r->exec));
+      delete r;
+      g_graphs.erase(g_graphs.begin() + i);
+      i--;
+      continue;
+    }
     if (same_grid(&r->key, g) && r->dt == dt && r->tol == log10_tol && r->R == integration_radius &&
         r->max_steps == max_steps)
       rg = r;
+  }
   if (!rg) {
     cudaGraph_t graph;
     const long long launches_before = g_launches;
     NRPYELL_CUDA(cudaStreamBeginCapture(stream(), cudaStreamCaptureModeThreadLocal));
     for (int k = 0; k < kStepsPerGraph; k++) {
-      FusedArgs a1 = fused_args(g, rt, bt, w, dt, 1, w->state + 1);
+      FusedArgs a1 = fused_args(g, rt, bt, w, s, dt, 1, w->state + 1);
       a1.lt = lt;
       launch_fused_substep<double>(1, a1);
       launch_relax_check(nblk, s, lt->volume, log10_tol, max_steps, w->history, w->state);
-      for (int st = 2; st <= 4; st++) launch_fused_substep<double>(st, fused_args(g, rt, bt, w, dt, st, w->state + 1));
+      for (int st = 2; st <= 4; st++)
+        launch_fused_substep<double>(st, fused_args(g, rt, bt, w, s, dt, st, w->state + 1));
     }
     NRPYELL_CUDA(cudaStreamEndCapture(stream(), &graph));
     g_launches = launches_before;  // captured launches run when the graph does
@@ -550,6 +585,8 @@ int nrpyell_relax(griddata_struct* g, const REAL dt, const REAL log10_tol, const
     rg->tol = log10_tol;
     rg->R = integration_radius;
     rg->max_steps = max_steps;
+    rg->scratch_gen = scratch_generation();
+    rg->work_gen = g_work_generation;
     NRPYELL_CUDA(cudaGraphInstantiate(&rg->exec, graph, 0));
     NRPYELL_CUDA(cudaGraphDestroy(graph));
     g_graphs.push_back(rg);

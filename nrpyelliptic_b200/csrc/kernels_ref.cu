@@ -254,6 +254,9 @@ __global__ void k_extrap_layer(Dims d, const OuterPoint* __restrict__ pts, int n
   const OuterPoint q = pts[t];
   const int F0 = q.i0n - q.i0, F1 = q.i1n - q.i1, F2 = q.i2n - q.i2;
   const int N0 = d.N0, N1 = d.N1;
+  // the three points towards the interior must lie on the grid
+  const int j0 = q.i0 + 3 * F0, j1 = q.i1 + 3 * F1, j2 = q.i2 + 3 * F2;
+  if (j0 < 0 || j0 >= N0 || j1 < 0 || j1 >= N1 || j2 < 0 || j2 >= d.N2) return;
   const long long i1d = q.idx3_int;
   const long long i2d = (q.i0 + 2 * F0) + (long long)N0 * ((q.i1 + 2 * F1) + (long long)N1 * (q.i2 + 2 * F2));
   const long long i3d = (q.i0 + 3 * F0) + (long long)N0 * ((q.i1 + 3 * F1) + (long long)N1 * (q.i2 + 3 * F2));

@@ -321,8 +321,12 @@ L2Tables* get_l2_tables(const paramstruct* p, REAL* NRPYELL_RESTRICT const xx[3]
   return t;
 }
 
+static int g_scratch_generation = 0;
+int scratch_generation() { return g_scratch_generation; }
+
 Scratch* get_scratch(int n_partials) {
   if (g_scratch && g_scratch->n_partials >= n_partials) return g_scratch;
+  g_scratch_generation++;  // graphs captured with the old buffer are stale
   if (g_scratch) {
     NRPYELL_CUDA(cudaStreamSynchronize(stream()));
     NRPYELL_CUDA(cudaFree(g_scratch->base));

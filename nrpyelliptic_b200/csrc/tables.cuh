@@ -102,6 +102,10 @@ struct Scratch {
   int* flags;        // [8]
   void* base;
 };
+// Returns scratch with at least n_partials partial-sum slots.  Never call it
+// while a stream is being captured: growing the buffer allocates.
 Scratch* get_scratch(int n_partials);
+// Incremented whenever the scratch buffer is reallocated.
+int scratch_generation();
 
 }  // namespace nrpyell
