@@ -109,6 +109,13 @@ int nrpyell_get_step_mode(void);
  * away.  nrpyell_set_async(1) lets them return after enqueueing; the caller
  * then orders host access with nrpyell_synchronize(). */
 void nrpyell_set_async(int enable);
+/* Tile shape of the fused RK4 substep kernel.  By default the library times
+ * every shape on the caller's grid the first time a grid size is stepped
+ * and keeps the fastest.  nrpyell_set_tile(t) forces shape t (-1: autotune);
+ * nrpyell_get_tile reports the shape in use for a grid (block 32 x by threads,
+ * `planes` consecutive i2 planes per thread), -1 if not tuned yet. */
+void nrpyell_set_tile(int tile);
+int nrpyell_get_tile(const paramstruct *params, int fp32, int *bx, int *by, int *planes);
 /* Selects the CUDA device used by every later call (default: device 0).
  * Call before any other GPU work in the process. */
 int nrpyell_set_device(int device);

@@ -5,6 +5,7 @@
 #include <stdlib.h>
 #include <string.h>
 
+#include <algorithm>
 #include <string>
 #include <vector>
 
@@ -102,15 +103,14 @@ static void mol_step_reference_order(griddata_struct* g, double dt) {
   }
 }
 
-// Scratch for the fused path: the face buffer (RHS on the last interior
-// plane, both gridfunctions) and the driver state.
+// Driver state of the fused path, per grid size.
 struct FusedWork {
   Dims d;
-  void* face;
   int* state;        // [0] n, [1] done, [2] converged
   int* zero_flag;    // always 0 (MoL_step_forward_in_time runs unconditionally)
   double* history;
   int history_len;
+  int tile[2];       // autotuned tile shape for FP64 / FP32, -1 = not yet tuned
 };
 static std::vector<FusedWork*> g_work;
 static int g_work_generation = 0;  // bumped when a work buffer is reallocated
@@ -130,7 +130,7 @@ static FusedWork* get_work(const Dims& d, int history_len) {
     }
   FusedWork* w = new FusedWork();
   w->d = d;
-  NRPYELL_CUDA(cudaMalloc(&w->face, sizeof(double) * 2 * (size_t)d.Nxx1 * d.Nxx2));
+  w->tile[0] = w->tile[1] = -1;
   NRPYELL_CUDA(cudaMalloc(&w->state, sizeof(int) * 8));
   NRPYELL_CUDA(cudaMemset(w->state, 0, sizeof(int) * 8));
   w->zero_flag = w->state + 4;
@@ -142,7 +142,6 @@ static FusedWork* get_work(const Dims& d, int history_len) {
 
 static void release_work() {
   for (FusedWork* w : g_work) {
-    cudaFree(w->face);
     cudaFree(w->state);
     cudaFree(w->history);
     delete w;
@@ -154,14 +153,16 @@ static bool fused_ready(griddata_struct* g, RfmTables** rt, BcTables** bt) {
   const paramstruct* p = &g->params;
   *rt = get_rfm_tables(p, &g->rfmstruct);
   *bt = get_bc_tables(p, &g->bcstruct, g->xx);
-  return *rt && *bt && (*bt)->columns_ok && p->outer_bc_type == RADIATION_OUTER_BCS;
+  return *rt && *bt && (*bt)->columns_ok && (*bt)->analytic_ok && p->outer_bc_type == RADIATION_OUTER_BCS;
 }
 
-static FusedArgs fused_args(griddata_struct* g, RfmTables* rt, BcTables* bt, FusedWork* w, Scratch* s, double dt,
-                            int stage, const int* done) {
+static int g_forced_tile = -1;
+
+static SubstepArgs substep_args(griddata_struct* g, RfmTables* rt, BcTables* bt, FusedWork* w, Scratch* s,
+                                double dt, int stage, const int* done, int tile) {
   const paramstruct* p = &g->params;
   MoL_gridfunctions_struct* gf = &g->gridfuncs;
-  FusedArgs a;
+  SubstepArgs a;
   a.d = dims_of(p);
   double* S[4] = {gf->y_n_gfs, gf->k_odd_gfs, gf->k_even_gfs, gf->k_odd_gfs};
   double* O[4] = {gf->k_odd_gfs, gf->k_even_gfs, gf->k_odd_gfs, gf->y_n_gfs};
@@ -177,10 +178,57 @@ static FusedArgs fused_args(griddata_struct* g, RfmTables* rt, BcTables* bt, Fus
   a.rt = rt;
   a.bt = bt;
   a.lt = nullptr;
-  a.face = w->face;
   a.s = s;
+  a.state = w->state;
+  a.history = nullptr;
+  a.log10_tol = -1e300;
+  a.max_steps = 0;
   a.done = done;
+  a.tile = tile;
+  (void)w;
   return a;
+}
+
+static int max_interior_blocks(const Dims& d) {
+  int m = 0;
+  for (int t = 0; t < substep_num_tiles(); t++) m = std::max(m, substep_interior_blocks(d, t));
+  return m;
+}
+
+// Tile-shape autotuner: times the stage-2 fused substep (the most common
+// kind) for every tile shape on the caller's own buffers and keeps the
+// fastest, once per grid size and precision.  The timing launches write only
+// the running-total and k_even buffers, which every RK4 step overwrites
+// before reading.
+template <typename T>
+static int tuned_tile(griddata_struct* g, RfmTables* rt, BcTables* bt, FusedWork* w, Scratch* sc, double dt) {
+  const int which = sizeof(T) == 8 ? 0 : 1;
+  if (g_forced_tile >= 0) return g_forced_tile;
+  if (w->tile[which] >= 0) return w->tile[which];
+  cudaEvent_t e0, e1;
+  NRPYELL_CUDA(cudaEventCreate(&e0));
+  NRPYELL_CUDA(cudaEventCreate(&e1));
+  int best = 0;
+  float best_ms = 1e30f;
+  const int reps = 10;
+  for (int t = 0; t < substep_num_tiles(); t++) {
+    SubstepArgs a = substep_args(g, rt, bt, w, sc, dt, 2, w->zero_flag, t);
+    launch_substep<T>(2, a);  // warm-up
+    NRPYELL_CUDA(cudaEventRecord(e0, stream()));
+    for (int i = 0; i < reps; i++) launch_substep<T>(2, a);
+    NRPYELL_CUDA(cudaEventRecord(e1, stream()));
+    NRPYELL_CUDA(cudaEventSynchronize(e1));
+    float ms = 0.0f;
+    NRPYELL_CUDA(cudaEventElapsedTime(&ms, e0, e1));
+    if (ms < best_ms) {
+      best_ms = ms;
+      best = t;
+    }
+  }
+  NRPYELL_CUDA(cudaEventDestroy(e0));
+  NRPYELL_CUDA(cudaEventDestroy(e1));
+  w->tile[which] = best;
+  return best;
 }
 
 static void mol_step_fused(griddata_struct* g, double dt) {
@@ -192,8 +240,12 @@ static void mol_step_fused(griddata_struct* g, double dt) {
   }
   const Dims d = dims_of(&g->params);
   FusedWork* w = get_work(d, 16);
-  Scratch* sc = get_scratch(fused_interior_blocks(d));
-  for (int s = 1; s <= 4; s++) launch_fused_substep<double>(s, fused_args(g, rt, bt, w, sc, dt, s, w->zero_flag));
+  Scratch* sc = get_scratch(max_interior_blocks(d));
+  const int tile = tuned_tile<double>(g, rt, bt, w, sc, dt);
+  for (int s = 1; s <= 4; s++) launch_substep<double>(s, substep_args(g, rt, bt, w, sc, dt, s, w->zero_flag, tile));
+  // the fused kernels read ghost values from their sources; give y_n the
+  // ghost zones the reference's all-points update leaves in it
+  launch_ghost_fill<double>(d, bt, g->gridfuncs.y_n_gfs);
 }
 
 static bool check_gridfuncs(const MoL_gridfunctions_struct* gf) {
@@ -213,6 +265,7 @@ struct RelaxGraph {
   double dt, tol, R;
   int max_steps;
   int scratch_gen, work_gen;  // buffers the graph was captured with
+  int tile;
   cudaGraphExec_t exec;
   size_t nodes;
 };
@@ -280,6 +333,18 @@ int nrpyell_abi_layout(int* out, int n) {
 
 void nrpyell_set_step_mode(int mode) { g_step_mode = mode; }
 void nrpyell_set_async(int enable) { g_async = enable != 0; }
+
+void nrpyell_set_tile(int tile) { g_forced_tile = (tile >= 0 && tile < substep_num_tiles()) ? tile : -1; }
+
+int nrpyell_get_tile(const paramstruct* params, int fp32, int* bx, int* by, int* planes) {
+  const Dims d = dims_of(params);
+  int tile = g_forced_tile;
+  if (tile < 0)
+    for (FusedWork* w : g_work)
+      if (w->d.N0 == d.N0 && w->d.N1 == d.N1 && w->d.N2 == d.N2) tile = w->tile[fp32 ? 1 : 0];
+  if (tile >= 0 && bx && by && planes) substep_tile_shape(tile, bx, by, planes);
+  return tile;
+}
 int nrpyell_get_step_mode(void) { return g_step_mode; }
 
 int nrpyell_set_device(int device) {
@@ -334,7 +399,8 @@ int nrpyell_time_fused(griddata_struct* g, const REAL dt, const int stage, const
   }
   const Dims d = dims_of(&g->params);
   FusedWork* w = get_work(d, 16);
-  Scratch* sc = get_scratch(fused_interior_blocks(d));
+  Scratch* sc = get_scratch(max_interior_blocks(d));
+  const int tile = tuned_tile<double>(g, rt, bt, w, sc, dt);
   cudaEvent_t e0, e1;
   NRPYELL_CUDA(cudaEventCreate(&e0));
   NRPYELL_CUDA(cudaEventCreate(&e1));
@@ -345,10 +411,10 @@ int nrpyell_time_fused(griddata_struct* g, const REAL dt, const int stage, const
     NRPYELL_CUDA(cudaStreamBeginCapture(stream(), cudaStreamCaptureModeThreadLocal));
     for (int i = 0; i < n_iter; i++) {
       if (which == 0) {
-        launch_fused_interior_only<double>(stage, fused_args(g, rt, bt, w, sc, dt, stage, w->zero_flag));
+        launch_substep<double>(stage, substep_args(g, rt, bt, w, sc, dt, stage, w->zero_flag, tile));
       } else {
         for (int s = 1; s <= 4; s++)
-          launch_fused_substep<double>(s, fused_args(g, rt, bt, w, sc, dt, s, w->zero_flag));
+          launch_substep<double>(s, substep_args(g, rt, bt, w, sc, dt, s, w->zero_flag, tile));
       }
     }
     NRPYELL_CUDA(cudaStreamEndCapture(stream(), &graph));
@@ -544,8 +610,8 @@ int nrpyell_relax(griddata_struct* g, const REAL dt, const REAL log10_tol, const
   if (!lt) return -1;
   const Dims d = dims_of(&g->params);
   FusedWork* w = get_work(d, max_steps + 1);
-  const int nblk = fused_interior_blocks(d);
-  Scratch* s = get_scratch(nblk);
+  Scratch* s = get_scratch(max_interior_blocks(d));
+  const int tile = tuned_tile<double>(g, rt, bt, w, s, dt);
 
   RelaxGraph* rg = nullptr;
   for (size_t i = 0; i < g_graphs.size(); i++) {
@@ -559,7 +625,7 @@ int nrpyell_relax(griddata_struct* g, const REAL dt, const REAL log10_tol, const
       continue;
     }
     if (same_grid(&r->key, g) && r->dt == dt && r->tol == log10_tol && r->R == integration_radius &&
-        r->max_steps == max_steps)
+        r->max_steps == max_steps && r->tile == tile)
       rg = r;
   }
   if (!rg) {
@@ -567,12 +633,15 @@ int nrpyell_relax(griddata_struct* g, const REAL dt, const REAL log10_tol, const
     const long long launches_before = g_launches;
     NRPYELL_CUDA(cudaStreamBeginCapture(stream(), cudaStreamCaptureModeThreadLocal));
     for (int k = 0; k < kStepsPerGraph; k++) {
-      FusedArgs a1 = fused_args(g, rt, bt, w, s, dt, 1, w->state + 1);
+      // stage 1 also evaluates the residual of y_n and runs the stop test
+      SubstepArgs a1 = substep_args(g, rt, bt, w, s, dt, 1, w->state + 1, tile);
       a1.lt = lt;
-      launch_fused_substep<double>(1, a1);
-      launch_relax_check(nblk, s, lt->volume, log10_tol, max_steps, w->history, w->state);
+      a1.history = w->history;
+      a1.log10_tol = log10_tol;
+      a1.max_steps = max_steps;
+      launch_substep<double>(1, a1);
       for (int st = 2; st <= 4; st++)
-        launch_fused_substep<double>(st, fused_args(g, rt, bt, w, s, dt, st, w->state + 1));
+        launch_substep<double>(st, substep_args(g, rt, bt, w, s, dt, st, w->state + 1, tile));
     }
     NRPYELL_CUDA(cudaStreamEndCapture(stream(), &graph));
     g_launches = launches_before;  // captured launches run when the graph does
@@ -587,6 +656,7 @@ int nrpyell_relax(griddata_struct* g, const REAL dt, const REAL log10_tol, const
     rg->max_steps = max_steps;
     rg->scratch_gen = scratch_generation();
     rg->work_gen = g_work_generation;
+    rg->tile = tile;
     NRPYELL_CUDA(cudaGraphInstantiate(&rg->exec, graph, 0));
     NRPYELL_CUDA(cudaGraphDestroy(graph));
     g_graphs.push_back(rg);
@@ -614,6 +684,8 @@ int nrpyell_relax(griddata_struct* g, const REAL dt, const REAL log10_tol, const
     }
     if (!status_ok()) return -1;
   }
+  // ghost zones of the solution, as the reference's all-points update leaves them
+  launch_ghost_fill<double>(d, bt, g->gridfuncs.y_n_gfs);
   NRPYELL_CUDA(cudaStreamSynchronize(stream()));
   int st[4];
   NRPYELL_CUDA(cudaMemcpy(st, w->state, sizeof(st), cudaMemcpyDeviceToHost));

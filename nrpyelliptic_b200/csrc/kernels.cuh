@@ -20,8 +20,9 @@ void launch_rk_update_ref(int stage, long long n, double dt, const double* k, co
 // Deterministic weighted sum of g^2 over the interior: result[0] = sum w g^2.
 void launch_l2_sum(const Dims& d, const L2Tables* lt, const double* g, Scratch* s);
 
-// ---- fused kernels (kernels_fused.cu) ----
-struct FusedArgs {
+// ---- fused substep kernel (kernels_fused.cu) ----
+// Requires BcTables::columns_ok && BcTables::analytic_ok.
+struct SubstepArgs {
   Dims d;
   const void* S;      // stage input state (uu, vv)
   const void* y;      // y_n
@@ -31,20 +32,25 @@ struct FusedArgs {
   double dt, eta, cOB[2];
   const RfmTables* rt;
   const BcTables* bt;
-  const L2Tables* lt;  // non-null: accumulate the residual's weighted L2 sum (stage 1)
-  void* face;          // [2][Nxx1*Nxx2] RHS on the last interior plane
+  // Stop test at stage 1 (relaxation driver); lt == nullptr: none.  The last
+  // interior block writes log10 L2 to history[state[0]] and updates state:
+  // [0] n, [1] done, [2] converged.
+  const L2Tables* lt;
   Scratch* s;
-  const int* done;     // device flag; kernels return immediately when *done != 0
+  int* state;
+  double* history;
+  double log10_tol;
+  int max_steps;
+  const int* done;  // kernels return at entry when *done != 0
+  int tile;         // tile shape index (autotuned)
 };
 template <typename T>
-void launch_fused_substep(int stage, const FusedArgs& a);
-// Only the interior kernel of a stage (timing helper).
+void launch_substep(int stage, const SubstepArgs& a);
+// Copies inner ghost points of gfs (2 gridfunctions) from their sources.
 template <typename T>
-void launch_fused_interior_only(int stage, const FusedArgs& a);
-// L2 finalisation for the relaxation driver: reads the partial sums written by
-// the stage-1 kernel, stores log10 L2 into history[n], and sets the done flag.
-void launch_relax_check(int nblocks, Scratch* s, double volume, double log10_tol, int max_steps, double* history,
-                        int* state);
-int fused_interior_blocks(const Dims& d);
+void launch_ghost_fill(const Dims& d, const BcTables* bt, void* gfs);
+int substep_num_tiles();
+void substep_tile_shape(int tile, int* bx, int* by, int* p);
+int substep_interior_blocks(const Dims& d, int tile);
 
 }  // namespace nrpyell

@@ -269,27 +269,7 @@ void nrpyell_bcstruct_set_up(const paramstruct *p, bc_struct *bc) {
   const int Nxx[3] = {p->Nxx0, p->Nxx1, p->Nxx2};
   nrpyell_set_Nxx_dxx_invdx_params__and__xx(0, Nxx, &q, xx);
 
-  auto map_point = [&](int i0, int i1, int i2, int out[3]) {
-    int shift = 0;
-    if (i0 < NGHOSTS) {
-      i0 = 2 * NGHOSTS - 1 - i0;
-      shift ^= 1;
-    }
-    if (i1 < NGHOSTS) {
-      i1 = 2 * NGHOSTS - 1 - i1;
-      shift ^= 1;
-    } else if (i1 >= NGHOSTS + Nxx1) {
-      i1 = 2 * (NGHOSTS + Nxx1) - 1 - i1;
-      shift ^= 1;
-    }
-    int j = i2 - NGHOSTS;  // interior index in [0, Nxx2) after wrapping
-    if (shift) j += Nxx2 / 2;
-    j %= Nxx2;
-    if (j < 0) j += Nxx2;
-    out[0] = i0;
-    out[1] = i1;
-    out[2] = j + NGHOSTS;
-  };
+  auto map_point = [&](int i0, int i1, int i2, int out[3]) { symtp_ghost_source(i0, i1, i2, Nxx1, Nxx2, out); };
   auto interior = [&](int i0, int i1, int i2) {
     return i0 >= NGHOSTS && i0 < N0 - NGHOSTS && i1 >= NGHOSTS && i1 < N1 - NGHOSTS && i2 >= NGHOSTS &&
            i2 < N2 - NGHOSTS;

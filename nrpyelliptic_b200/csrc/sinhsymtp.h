@@ -109,4 +109,35 @@ NRPYELL_HD void symtp_ds(double AMAX, double SINHWAA, double bScale, double dxx0
   ds[2] = dxx2 * s1 * Aden * sh;
 }
 
+// Source point of a ghost point on the cell-centred SymTP grid (NGHOSTS = 5
+// ghost layers around Nxx0 x Nxx1 x Nxx2 interior points):
+//   xx0 < 0          -> xx0' = -xx0, xx2' = xx2 + pi   (A -> -A flips x and y)
+//   xx1 < 0 or > pi  -> xx1' = -xx1 or 2pi - xx1, xx2' = xx2 + pi
+//   xx2 outside [-pi, pi) -> wrap by 2pi
+// The outer xx0 face has no image: a point there maps to itself unless one of
+// its other coordinates is reflected.  This is the round trip
+// xx -> Cartesian -> xx of bcstruct_set_up.c:27-194 written on indices.
+NRPYELL_HD void symtp_ghost_source(int i0, int i1, int i2, int Nxx1, int Nxx2, int out[3]) {
+  const int NG = 5;
+  int shift = 0;
+  if (i0 < NG) {
+    i0 = 2 * NG - 1 - i0;
+    shift ^= 1;
+  }
+  if (i1 < NG) {
+    i1 = 2 * NG - 1 - i1;
+    shift ^= 1;
+  } else if (i1 >= NG + Nxx1) {
+    i1 = 2 * (NG + Nxx1) - 1 - i1;
+    shift ^= 1;
+  }
+  int j = i2 - NG;
+  if (shift) j += Nxx2 / 2;
+  j %= Nxx2;
+  if (j < 0) j += Nxx2;
+  out[0] = i0;
+  out[1] = i1;
+  out[2] = j + NG;
+}
+
 #endif

@@ -194,6 +194,19 @@ BcTables* get_bc_tables(const paramstruct* p, const bc_struct* bc, REAL* NRPYELL
     par[i] = bc->inner_bc_array[i].parity[0];
   }
   t->n_inner = ni;
+  {
+    // Inner map == SymTP reflections, and inner + pure outer cover every ghost point.
+    bool ok = ((long long)ni == d.Ntot - (long long)d.Nxx0 * d.Nxx1 * d.Nxx2 - (long long)NGHOSTS * d.Nxx1 * d.Nxx2) &&
+              d.Nxx2 % 2 == 0 && d.Nxx2 >= NGHOSTS;
+    for (int i = 0; i < ni && ok; i++) {
+      const int dst = inner[i].x;
+      const int i0 = dst % N0, i1 = (dst / N0) % N1, i2 = dst / (N0 * N1);
+      int m[3];
+      symtp_ghost_source(i0, i1, i2, d.Nxx1, d.Nxx2, m);
+      ok = (m[0] + N0 * (m[1] + N1 * m[2]) == inner[i].y) && par[i] == 1;
+    }
+    t->analytic_ok = ok;
+  }
 
   // Generic outer lists with precomputed geometry.
   std::vector<OuterPoint> outer;

@@ -74,6 +74,10 @@ struct BcTables {
   // fused-path column form: every pure outer point lies on the x0max face,
   // layer gz = i0 == N0-NGHOSTS+gz over all interior (i1,i2)
   bool columns_ok;
+  // every inner point copies from the SymTP reflection of itself
+  // (symtp_ghost_source), so kernels may read ghost values straight from
+  // their source points instead of from the ghost zones
+  bool analytic_ok;
   // geometry for the column form, [6][N1]: j=0 is the last interior plane,
   // j=1..5 the outer layers; arrays r, dx0dr, dx1dr
   double* colgeo;
