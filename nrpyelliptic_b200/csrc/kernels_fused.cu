@@ -35,7 +35,7 @@ struct SubDev {
   int N0, N1, Nxx0, Nxx1, Nxx2, half2;
   long long N01, Ntot;
   int tiles0, tiles1, tiles2;  // interior tile grid
-  int n_int_blocks, ncol;
+  int n_int_blocks, ncol, n_col_blocks;
   const T* __restrict__ S;     // stage input
   const T* y;                  // y_n (aliases out at stage 4)
   T* acc;
@@ -155,9 +155,11 @@ __global__ void __launch_bounds__(32 * BY) k_substep(SubDev<T> a) {
   __shared__ double drf[CB][2][6], fvs[CB][2][6], kl[CB][2], kk[CB][2][5];
   if (*a.done) return;
   const int tid = threadIdx.x;
-  if ((int)blockIdx.x < a.n_int_blocks) {
+  // Column blocks come first in the launch order: their dependent load
+  // chains then overlap with the interior blocks instead of forming a tail.
+  if ((int)blockIdx.x >= a.n_col_blocks) {
     // ------------------------------------------------------------ interior
-    const int b = blockIdx.x;
+    const int b = blockIdx.x - a.n_col_blocks;
     const int t0 = b % a.tiles0, t1 = (b / a.tiles0) % a.tiles1, t2 = b / (a.tiles0 * a.tiles1);
     const int i0 = t0 * 32 + (tid & 31) + NGHOSTS;
     const int i1 = t1 * BY + (tid >> 5) + NGHOSTS;
@@ -252,7 +254,7 @@ __global__ void __launch_bounds__(32 * BY) k_substep(SubDev<T> a) {
   // gridfunction g = r / 6 (point jj is i0 = N0-6+jj; jj = 0 is the last
   // interior plane, jj = 1..5 the outer layers 0..4); r == 12 -> RHS at the
   // last interior point.
-  const int cb = blockIdx.x - a.n_int_blocks;
+  const int cb = blockIdx.x;
   const int c = tid / kColThreadsPerColumn, r = tid % kColThreadsPerColumn;
   const int colid = cb * CB + c;
   const bool live = colid < a.ncol;
@@ -425,8 +427,8 @@ static void launch_one(const SubstepArgs& a) {
   SubDev<T> f = make_dev<T>(a);
   constexpr int NT = 32 * BY;
   constexpr int CB = NT / kColThreadsPerColumn;
-  const int ncb = (f.ncol + CB - 1) / CB;
-  NRPYELL_LAUNCH((k_substep<T, STAGE, RESID, BY, P>), f.n_int_blocks + ncb, NT, 0, f);
+  f.n_col_blocks = (f.ncol + CB - 1) / CB;
+  NRPYELL_LAUNCH((k_substep<T, STAGE, RESID, BY, P>), f.n_int_blocks + f.n_col_blocks, NT, 0, f);
 }
 
 template <typename T, int STAGE, bool RESID>
