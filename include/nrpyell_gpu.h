@@ -73,6 +73,18 @@ void residual_all_points(const paramstruct *NRPYELL_RESTRICT params, const rfm_s
 REAL L2_norm_of_gf(const paramstruct *NRPYELL_RESTRICT params, const int gf_index, const REAL integration_radius,
                    REAL *NRPYELL_RESTRICT xx[3], const REAL *NRPYELL_RESTRICT in_gf);
 
+/* Same result as L2_norm_of_gf, for callers that may not allocate device
+ * memory (no counterpart in the reference): all working memory is one
+ * fixed-size array in the library (37.5 KB per GPU, held until exit), so no
+ * cudaMalloc/cudaFree is ever called.  Grids are limited to 2048 x 2048
+ * points in xx0 x xx1 (ghosts included); larger ones are rejected with an
+ * error and NaN.  Calls share the array: calls that overlap on the GPU race.
+ * The first call on a device looks the array up (cudaGetSymbolAddress) and
+ * should come before any stream capture. */
+REAL L2_norm_of_gf_noalloc(const paramstruct *NRPYELL_RESTRICT params, const int gf_index,
+                           const REAL integration_radius, REAL *NRPYELL_RESTRICT xx[3],
+                           const REAL *NRPYELL_RESTRICT in_gf);
+
 /* ---------------- Part 2: library extensions ---------------- */
 
 /* Status and error policy. */

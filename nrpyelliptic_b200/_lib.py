@@ -31,6 +31,7 @@ EXPORTS = {
     "apply_bcs_outerextrap_and_inner": (None, [P(abi.paramstruct), P(abi.bc_struct), PREAL]),
     "residual_all_points": (None, [P(abi.paramstruct), P(abi.rfm_struct), PREAL, PREAL, PREAL]),
     "L2_norm_of_gf": (C.c_double, [P(abi.paramstruct), C.c_int, C.c_double, XX, PREAL]),
+    "L2_norm_of_gf_noalloc": (C.c_double, [P(abi.paramstruct), C.c_int, C.c_double, XX, PREAL]),
     # extensions
     "nrpyell_last_status": (C.c_int, []),
     "nrpyell_last_error": (C.c_char_p, []),

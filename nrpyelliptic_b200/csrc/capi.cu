@@ -47,6 +47,8 @@ cudaStream_t stream() {
   return g_stream;
 }
 
+cudaStream_t existing_stream() { return g_stream; }
+
 void count_launch(int n) { g_launches += n; }
 
 bool check_device_pointer(const void* ptr, const char* what) {

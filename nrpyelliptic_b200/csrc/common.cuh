@@ -14,6 +14,9 @@ namespace nrpyell {
 void report_error(const char* file, int line, const char* what);
 bool status_ok();
 cudaStream_t stream();
+// The library's stream if it has been created, else the default stream (0);
+// never creates one.
+cudaStream_t existing_stream();
 void count_launch(int n = 1);
 
 #define NRPYELL_CUDA(call)                                                     \
