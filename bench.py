@@ -53,38 +53,6 @@ def parse():
     return ap.parse_args()
 
 
-class Dist:
-    def __init__(self):
-        self.rank = int(os.environ.get("RANK", "0"))
-        self.world = int(os.environ.get("WORLD_SIZE", "1"))
-        self.local_rank = int(os.environ.get("LOCAL_RANK", "0"))
-        self.torch = None
-        if self.world > 1:
-            import datetime
-
-            import torch
-            import torch.distributed as dist
-            self.torch = torch
-            torch.cuda.set_device(self.local_rank)
-            dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
-            self.dist = dist
-
-    def barrier(self):
-        if self.torch:
-            self.dist.barrier()
-
-    def max(self, x):
-        if not self.torch:
-            return x
-        t = self.torch.tensor([x], dtype=self.torch.float64, device="cuda")
-        self.dist.all_reduce(t, op=self.dist.ReduceOp.MAX)
-        return float(t.item())
-
-    def close(self):
-        if self.torch:
-            self.dist.destroy_process_group()
-
-
 class Clocks:
     """nvidia-smi samples during the timed region."""
     Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
@@ -379,8 +347,9 @@ def run_ours(args, dist):
 
 
 def main():
+    from nrpyelliptic_b200.replicas import Replicas
     args = parse()
-    dist = Dist()
+    dist = Replicas()
     try:
         if args.impl == "reference":
             run_reference(args, dist)
