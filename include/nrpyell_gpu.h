@@ -172,6 +172,21 @@ REAL nrpyell_compute_wavespeed_at_OB(const paramstruct *params, const REAL *auxe
 int nrpyell_relax(griddata_struct *griddata, const REAL dt, const REAL log10_tol, const int max_steps,
                   const REAL integration_radius, int *steps_taken, REAL *final_log10_l2, REAL *history);
 
+/* Mixed-precision relaxation: FP32 storage and arithmetic (the residual norm
+ * accumulated in FP64) from the initial y_n until log10 L2 <= log10_switch or
+ * the residual stalls -- its best value so far has not dropped below
+ * stall_factor (e.g. 0.98) times itself for stall_window steps; the
+ * relaxation residual oscillates, so only the running minimum is judged, and
+ * only once it is within two decades of log10_switch --
+ * then FP64 from that state to
+ * log10_tol.  steps_fp32 / steps_fp64 receive the RK4 steps of each phase;
+ * history (nullable) log10 L2 per evaluated step (phase-2 values overwrite
+ * the phase-1 value at the switch step).  Returns as nrpyell_relax. */
+int nrpyell_relax_mixed(griddata_struct *griddata, const REAL dt, const REAL log10_tol, const REAL log10_switch,
+                        const int stall_window, const REAL stall_factor, const int max_steps,
+                        const REAL integration_radius, int *steps_fp32, int *steps_fp64, REAL *final_log10_l2,
+                        REAL *history);
+
 /* The same solve with host buffers: copies auxevol_host (3 gfs) and
  * y_n_host (2 gfs, the initial guess) to the device, relaxes, copies the
  * solution back into y_n_host. */

@@ -18,7 +18,7 @@ CSRC = os.path.join(HERE, "csrc")
 INCLUDE = os.path.join(ROOT, "include")
 LIB = os.path.join(HERE, "libnrpyell_gpu.so")
 
-SOURCES = ["capi.cu", "tables.cu", "kernels_ref.cu", "kernels_fused.cu", "noalloc.cu", "setup.cpp"]
+SOURCES = ["capi.cu", "driver.cu", "tables.cu", "kernels_ref.cu", "kernels_fused.cu", "noalloc.cu", "setup.cpp"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 
 

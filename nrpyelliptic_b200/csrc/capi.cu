@@ -9,7 +9,7 @@
 #include <string>
 #include <vector>
 
-#include "kernels.cuh"
+#include "driver.cuh"
 
 namespace nrpyell {
 
@@ -50,6 +50,8 @@ cudaStream_t stream() {
 cudaStream_t existing_stream() { return g_stream; }
 
 void count_launch(int n) { g_launches += n; }
+long long launch_count() { return g_launches; }
+void set_launch_count(long long n) { g_launches = n; }
 
 bool check_device_pointer(const void* ptr, const char* what) {
   char msg[256];
@@ -105,146 +107,32 @@ static void mol_step_reference_order(griddata_struct* g, double dt) {
   }
 }
 
-// Driver state of the fused path, per grid size.
-struct FusedWork {
-  Dims d;
-  int* state;        // [0] n, [1] done, [2] converged
-  int* zero_flag;    // always 0 (MoL_step_forward_in_time runs unconditionally)
-  double* history;
-  int history_len;
-  int tile[2];       // autotuned tile shape for FP64 / FP32, -1 = not yet tuned
-};
-static std::vector<FusedWork*> g_work;
-static int g_work_generation = 0;  // bumped when a work buffer is reallocated
-
-// Never call while a stream is being captured (it may allocate).
-static FusedWork* get_work(const Dims& d, int history_len) {
-  for (FusedWork* w : g_work)
-    if (w->d.Nxx1 == d.Nxx1 && w->d.Nxx2 == d.Nxx2 && w->d.N0 == d.N0 && w->d.N1 == d.N1 && w->d.N2 == d.N2) {
-      if (w->history_len < history_len) {
-        g_work_generation++;
-        NRPYELL_CUDA(cudaStreamSynchronize(stream()));
-        NRPYELL_CUDA(cudaFree(w->history));
-        NRPYELL_CUDA(cudaMalloc(&w->history, sizeof(double) * history_len));
-        w->history_len = history_len;
-      }
-      return w;
-    }
-  FusedWork* w = new FusedWork();
-  w->d = d;
-  w->tile[0] = w->tile[1] = -1;
-  NRPYELL_CUDA(cudaMalloc(&w->state, sizeof(int) * 8));
-  NRPYELL_CUDA(cudaMemset(w->state, 0, sizeof(int) * 8));
-  w->zero_flag = w->state + 4;
-  w->history_len = history_len > 16 ? history_len : 16;
-  NRPYELL_CUDA(cudaMalloc(&w->history, sizeof(double) * w->history_len));
-  g_work.push_back(w);
-  return w;
-}
-
-static void release_work() {
-  for (FusedWork* w : g_work) {
-    cudaFree(w->state);
-    cudaFree(w->history);
-    delete w;
-  }
-  g_work.clear();
-}
-
-static bool fused_ready(griddata_struct* g, RfmTables** rt, BcTables** bt) {
-  const paramstruct* p = &g->params;
-  *rt = get_rfm_tables(p, &g->rfmstruct);
-  *bt = get_bc_tables(p, &g->bcstruct, g->xx);
-  return *rt && *bt && (*bt)->columns_ok && (*bt)->analytic_ok && p->outer_bc_type == RADIATION_OUTER_BCS;
-}
-
-static int g_forced_tile = -1;
-
-static SubstepArgs substep_args(griddata_struct* g, RfmTables* rt, BcTables* bt, FusedWork* w, Scratch* s,
-                                double dt, int stage, const int* done, int tile) {
-  const paramstruct* p = &g->params;
-  MoL_gridfunctions_struct* gf = &g->gridfuncs;
-  SubstepArgs a;
-  a.d = dims_of(p);
-  double* S[4] = {gf->y_n_gfs, gf->k_odd_gfs, gf->k_even_gfs, gf->k_odd_gfs};
-  double* O[4] = {gf->k_odd_gfs, gf->k_even_gfs, gf->k_odd_gfs, gf->y_n_gfs};
-  a.S = S[stage - 1];
-  a.out = O[stage - 1];
-  a.y = gf->y_n_gfs;
-  a.acc = gf->y_nplus1_running_total_gfs;
-  a.aux = gf->auxevol_gfs;
-  a.dt = dt;
-  a.eta = p->eta_damping;
-  a.cOB[0] = p->uu_wavespeed_at_OB;
-  a.cOB[1] = p->vv_wavespeed_at_OB;
-  a.rt = rt;
-  a.bt = bt;
-  a.lt = nullptr;
-  a.s = s;
-  a.state = w->state;
-  a.history = nullptr;
-  a.log10_tol = -1e300;
-  a.max_steps = 0;
-  a.done = done;
-  a.tile = tile;
-  (void)w;
-  return a;
-}
-
-static int max_interior_blocks(const Dims& d) {
-  int m = 0;
-  for (int t = 0; t < substep_num_tiles(); t++) m = std::max(m, substep_interior_blocks(d, t));
-  return m;
-}
-
-// Tile-shape autotuner: times the stage-2 fused substep (the most common
-// kind) for every tile shape on the caller's own buffers and keeps the
-// fastest, once per grid size and precision.  The timing launches write only
-// the running-total and k_even buffers, which every RK4 step overwrites
-// before reading.
-template <typename T>
-static int tuned_tile(griddata_struct* g, RfmTables* rt, BcTables* bt, FusedWork* w, Scratch* sc, double dt) {
-  const int which = sizeof(T) == 8 ? 0 : 1;
-  if (g_forced_tile >= 0) return g_forced_tile;
-  if (w->tile[which] >= 0) return w->tile[which];
-  cudaEvent_t e0, e1;
-  NRPYELL_CUDA(cudaEventCreate(&e0));
-  NRPYELL_CUDA(cudaEventCreate(&e1));
-  int best = 0;
-  float best_ms = 1e30f;
-  const int reps = 10;
-  for (int t = 0; t < substep_num_tiles(); t++) {
-    SubstepArgs a = substep_args(g, rt, bt, w, sc, dt, 2, w->zero_flag, t);
-    launch_substep<T>(2, a);  // warm-up
-    NRPYELL_CUDA(cudaEventRecord(e0, stream()));
-    for (int i = 0; i < reps; i++) launch_substep<T>(2, a);
-    NRPYELL_CUDA(cudaEventRecord(e1, stream()));
-    NRPYELL_CUDA(cudaEventSynchronize(e1));
-    float ms = 0.0f;
-    NRPYELL_CUDA(cudaEventElapsedTime(&ms, e0, e1));
-    if (ms < best_ms) {
-      best_ms = ms;
-      best = t;
-    }
-  }
-  NRPYELL_CUDA(cudaEventDestroy(e0));
-  NRPYELL_CUDA(cudaEventDestroy(e1));
-  w->tile[which] = best;
-  return best;
+static RelaxParams relax_params(const paramstruct* p, double dt) {
+  RelaxParams rp;
+  memset(&rp, 0, sizeof(rp));  // graph keys compare the bytes
+  rp.dt = dt;
+  rp.eta = p->eta_damping;
+  rp.cOB[0] = p->uu_wavespeed_at_OB;
+  rp.cOB[1] = p->vv_wavespeed_at_OB;
+  rp.log10_tol = -1e300;
+  return rp;
 }
 
 static void mol_step_fused(griddata_struct* g, double dt) {
   RfmTables* rt;
   BcTables* bt;
-  if (!fused_ready(g, &rt, &bt)) {
+  if (!fused_ready(&g->params, &g->rfmstruct, &g->bcstruct, g->xx, &rt, &bt)) {
     mol_step_reference_order(g, dt);
     return;
   }
   const Dims d = dims_of(&g->params);
   FusedWork* w = get_work(d, 16);
   Scratch* sc = get_scratch(max_interior_blocks(d));
-  const int tile = tuned_tile<double>(g, rt, bt, w, sc, dt);
-  for (int s = 1; s <= 4; s++) launch_substep<double>(s, substep_args(g, rt, bt, w, sc, dt, s, w->zero_flag, tile));
+  const StateBuffers b = buffers_of(&g->gridfuncs);
+  const RelaxParams rp = relax_params(&g->params, dt);
+  const int tile = tuned_tile<double>(d, rt, bt, w, sc, b, rp);
+  for (int s = 1; s <= 4; s++)
+    launch_substep<double>(s, substep_args(d, rt, bt, sc, b, rp, s, w->zero_flag, w->state, tile));
   // the fused kernels read ghost values from their sources; give y_n the
   // ghost zones the reference's all-points update leaves in it
   launch_ghost_fill<double>(d, bt, g->gridfuncs.y_n_gfs);
@@ -257,43 +145,44 @@ static bool check_gridfuncs(const MoL_gridfunctions_struct* gf) {
          check_device_pointer(gf->auxevol_gfs, "auxevol_gfs");
 }
 
-// Graph-cached relaxation: a CUDA graph of kStepsPerGraph RK4 steps (each
-// preceded by the fused residual/L2 test) is replayed until the device-side
-// state says done.  Kernels after convergence return at entry.
-constexpr int kStepsPerGraph = 16;
-
-struct RelaxGraph {
-  griddata_struct key;
-  double dt, tol, R;
-  int max_steps;
-  int scratch_gen, work_gen;  // buffers the graph was captured with
-  int tile;
-  cudaGraphExec_t exec;
-  size_t nodes;
-};
-static std::vector<RelaxGraph*> g_graphs;
-
-static void release_graphs() {
-  for (RelaxGraph* r : g_graphs) {
-    cudaGraphExecDestroy(r->exec);
-    delete r;
-  }
-  g_graphs.clear();
-}
-
-static bool same_grid(const griddata_struct* a, const griddata_struct* b) {
-  return memcmp(&a->params, &b->params, sizeof(paramstruct)) == 0 && a->xx[0] == b->xx[0] && a->xx[1] == b->xx[1] &&
-         a->xx[2] == b->xx[2] && a->bcstruct.inner_bc_array == b->bcstruct.inner_bc_array &&
-         a->rfmstruct.f0_of_xx0 == b->rfmstruct.f0_of_xx0 &&
-         memcmp(&a->gridfuncs, &b->gridfuncs, sizeof(MoL_gridfunctions_struct)) == 0;
-}
-
 // The reference's functions return when their work is done, and callers such
 // as main.c read managed gridfunctions on the host right after a call; the
 // Part-1 entry points therefore wait for their kernels unless the caller
 // opted into asynchronous calls.
 static void finish_call() {
   if (!g_async) NRPYELL_CUDA(cudaStreamSynchronize(stream()));
+}
+
+// Common preparation of the fused relaxation drivers.
+struct RelaxSetup {
+  Dims d;
+  RfmTables* rt;
+  BcTables* bt;
+  L2Tables* lt;
+  FusedWork* w;
+  Scratch* s;
+};
+
+static int relax_prepare(griddata_struct* g, int max_steps, double R, RelaxSetup* out, const char* who) {
+  char msg[256];
+  if (max_steps < 0) {
+    snprintf(msg, sizeof(msg), "%s: max_steps < 0", who);
+    NRPYELL_FAIL(msg);
+    return -1;
+  }
+  if (!check_gridfuncs(&g->gridfuncs)) return -1;
+  if (!fused_ready(&g->params, &g->rfmstruct, &g->bcstruct, g->xx, &out->rt, &out->bt)) {
+    snprintf(msg, sizeof(msg),
+             "%s needs radiation outer BCs with the SymTP inner-boundary map and x0max-only pure outer points", who);
+    NRPYELL_FAIL(msg);
+    return -2;
+  }
+  out->lt = get_l2_tables(&g->params, g->xx, R);
+  if (!out->lt) return -1;
+  out->d = dims_of(&g->params);
+  out->w = get_work(out->d, max_steps + 1);
+  out->s = get_scratch(max_interior_blocks(out->d));
+  return status_ok() ? 0 : -1;
 }
 
 }  // namespace nrpyell
@@ -334,20 +223,16 @@ int nrpyell_abi_layout(int* out, int n) {
 }
 
 void nrpyell_set_step_mode(int mode) { g_step_mode = mode; }
+int nrpyell_get_step_mode(void) { return g_step_mode; }
 void nrpyell_set_async(int enable) { g_async = enable != 0; }
 
 void nrpyell_set_tile(int tile) { g_forced_tile = (tile >= 0 && tile < substep_num_tiles()) ? tile : -1; }
 
 int nrpyell_get_tile(const paramstruct* params, int fp32, int* bx, int* by, int* planes) {
-  const Dims d = dims_of(params);
-  int tile = g_forced_tile;
-  if (tile < 0)
-    for (FusedWork* w : g_work)
-      if (w->d.N0 == d.N0 && w->d.N1 == d.N1 && w->d.N2 == d.N2) tile = w->tile[fp32 ? 1 : 0];
+  int tile = g_forced_tile >= 0 ? g_forced_tile : find_tile(dims_of(params), fp32);
   if (tile >= 0 && bx && by && planes) substep_tile_shape(tile, bx, by, planes);
   return tile;
 }
-int nrpyell_get_step_mode(void) { return g_step_mode; }
 
 int nrpyell_set_device(int device) {
   NRPYELL_CUDA(cudaSetDevice(device));
@@ -395,14 +280,17 @@ int nrpyell_time_fused(griddata_struct* g, const REAL dt, const int stage, const
   if (!check_gridfuncs(&g->gridfuncs)) return -1;
   RfmTables* rt;
   BcTables* bt;
-  if (!fused_ready(g, &rt, &bt) || stage < 1 || stage > 4 || n_iter < 1) {
+  if (!fused_ready(&g->params, &g->rfmstruct, &g->bcstruct, g->xx, &rt, &bt) || stage < 1 || stage > 4 ||
+      n_iter < 1) {
     NRPYELL_FAIL("nrpyell_time_fused: fused path unavailable for this grid or bad arguments");
     return -2;
   }
   const Dims d = dims_of(&g->params);
   FusedWork* w = get_work(d, 16);
   Scratch* sc = get_scratch(max_interior_blocks(d));
-  const int tile = tuned_tile<double>(g, rt, bt, w, sc, dt);
+  const StateBuffers b = buffers_of(&g->gridfuncs);
+  const RelaxParams rp = relax_params(&g->params, dt);
+  const int tile = tuned_tile<double>(d, rt, bt, w, sc, b, rp);
   cudaEvent_t e0, e1;
   NRPYELL_CUDA(cudaEventCreate(&e0));
   NRPYELL_CUDA(cudaEventCreate(&e1));
@@ -413,10 +301,10 @@ int nrpyell_time_fused(griddata_struct* g, const REAL dt, const int stage, const
     NRPYELL_CUDA(cudaStreamBeginCapture(stream(), cudaStreamCaptureModeThreadLocal));
     for (int i = 0; i < n_iter; i++) {
       if (which == 0) {
-        launch_substep<double>(stage, substep_args(g, rt, bt, w, sc, dt, stage, w->zero_flag, tile));
+        launch_substep<double>(stage, substep_args(d, rt, bt, sc, b, rp, stage, w->zero_flag, w->state, tile));
       } else {
         for (int s = 1; s <= 4; s++)
-          launch_substep<double>(s, substep_args(g, rt, bt, w, sc, dt, s, w->zero_flag, tile));
+          launch_substep<double>(s, substep_args(d, rt, bt, sc, b, rp, s, w->zero_flag, w->state, tile));
       }
     }
     NRPYELL_CUDA(cudaStreamEndCapture(stream(), &graph));
@@ -540,8 +428,7 @@ void residual_all_points(const paramstruct* params, const rfm_struct* rfmstruct,
 }
 
 void apply_bcs_outerradiation_and_inner(const paramstruct* params, const bc_struct* bcstruct,
-                                        REAL* NRPYELL_RESTRICT xx[3],
-                                        const REAL custom_wavespeed[NUM_EVOL_GFS],
+                                        REAL* NRPYELL_RESTRICT xx[3], const REAL custom_wavespeed[NUM_EVOL_GFS],
                                         const REAL custom_f_infinity[NUM_EVOL_GFS], REAL* gfs, REAL* rhs_gfs) {
   if (!check_device_pointer(gfs, "gfs") || !check_device_pointer(rhs_gfs, "rhs_gfs")) return;
   BcTables* bt = get_bc_tables(params, bcstruct, xx);
@@ -580,8 +467,7 @@ void MoL_step_forward_in_time(griddata_struct* griddata, const REAL dt) {
 }
 
 REAL L2_norm_of_gf(const paramstruct* params, const int gf_index, const REAL integration_radius,
-                   REAL* NRPYELL_RESTRICT xx[3],
-                   const REAL* in_gf) {
+                   REAL* NRPYELL_RESTRICT xx[3], const REAL* in_gf) {
   if (!check_device_pointer(in_gf, "in_gf")) return NAN;
   L2Tables* lt = get_l2_tables(params, xx, integration_radius);
   if (!lt) return NAN;
@@ -595,111 +481,83 @@ REAL L2_norm_of_gf(const paramstruct* params, const int gf_index, const REAL int
   return log10(1e-16 + sqrt(sum / lt->volume));
 }
 
+// ---- relaxation drivers ----
 int nrpyell_relax(griddata_struct* g, const REAL dt, const REAL log10_tol, const int max_steps,
                   const REAL integration_radius, int* steps_taken, REAL* final_log10_l2, REAL* history) {
-  if (max_steps < 0) {
-    NRPYELL_FAIL("nrpyell_relax: max_steps < 0");
+  RelaxSetup su;
+  const int rc = relax_prepare(g, max_steps, integration_radius, &su, "nrpyell_relax");
+  if (rc) return rc;
+  const StateBuffers b = buffers_of(&g->gridfuncs);
+  RelaxParams rp = relax_params(&g->params, dt);
+  rp.log10_tol = log10_tol;
+  rp.max_steps = max_steps;
+  const int tile = tuned_tile<double>(su.d, su.rt, su.bt, su.w, su.s, b, rp);
+  const RelaxResult r = relax_loop<double>(su.d, su.rt, su.bt, su.lt, su.w, su.s, tile, b, rp);
+  // ghost zones of the solution, as the reference's all-points update leaves them
+  launch_ghost_fill<double>(su.d, su.bt, g->gridfuncs.y_n_gfs);
+  if (history)
+    NRPYELL_CUDA(cudaMemcpyAsync(history, su.w->history, sizeof(double) * (r.steps + 1), cudaMemcpyDeviceToHost,
+                                 stream()));
+  NRPYELL_CUDA(cudaStreamSynchronize(stream()));
+  if (!status_ok()) return -1;
+  if (steps_taken) *steps_taken = r.steps;
+  if (final_log10_l2) *final_log10_l2 = r.last_log10_l2;
+  return r.converged ? 0 : 1;
+}
+
+int nrpyell_relax_mixed(griddata_struct* g, const REAL dt, const REAL log10_tol, const REAL log10_switch,
+                        const int stall_window, const REAL stall_factor, const int max_steps,
+                        const REAL integration_radius, int* steps_fp32, int* steps_fp64, REAL* final_log10_l2,
+                        REAL* history) {
+  RelaxSetup su;
+  const int rc = relax_prepare(g, max_steps, integration_radius, &su, "nrpyell_relax_mixed");
+  if (rc) return rc;
+  if (!(stall_factor > 0.0 && stall_factor < 1.0) || stall_window < 0) {
+    NRPYELL_FAIL("nrpyell_relax_mixed: need 0 < stall_factor < 1 and stall_window >= 0");
     return -1;
   }
-  if (!check_gridfuncs(&g->gridfuncs)) return -1;
-  RfmTables* rt;
-  BcTables* bt;
-  if (!fused_ready(g, &rt, &bt)) {
-    NRPYELL_FAIL("nrpyell_relax needs radiation outer BCs whose pure outer points form the x0max face");
-    return -2;
-  }
-  L2Tables* lt = get_l2_tables(&g->params, g->xx, integration_radius);
-  if (!lt) return -1;
-  const Dims d = dims_of(&g->params);
-  FusedWork* w = get_work(d, max_steps + 1);
-  Scratch* s = get_scratch(max_interior_blocks(d));
-  const int tile = tuned_tile<double>(g, rt, bt, w, s, dt);
-
-  RelaxGraph* rg = nullptr;
-  for (size_t i = 0; i < g_graphs.size(); i++) {
-    RelaxGraph* r = g_graphs[i];
-    if (r->scratch_gen != scratch_generation() || r->work_gen != g_work_generation) {
-      // captured with buffers that have since been reallocated
-      NRPYELL_CUDA(cudaGraphExecDestroy(r->exec));
-      delete r;
-      g_graphs.erase(g_graphs.begin() + i);
-      i--;
-      continue;
-    }
-    if (same_grid(&r->key, g) && r->dt == dt && r->tol == log10_tol && r->R == integration_radius &&
-        r->max_steps == max_steps && r->tile == tile)
-      rg = r;
-  }
-  if (!rg) {
-    cudaGraph_t graph;
-    const long long launches_before = g_launches;
-    NRPYELL_CUDA(cudaStreamBeginCapture(stream(), cudaStreamCaptureModeThreadLocal));
-    for (int k = 0; k < kStepsPerGraph; k++) {
-      // stage 1 also evaluates the residual of y_n and runs the stop test
-      SubstepArgs a1 = substep_args(g, rt, bt, w, s, dt, 1, w->state + 1, tile);
-      a1.lt = lt;
-      a1.history = w->history;
-      a1.log10_tol = log10_tol;
-      a1.max_steps = max_steps;
-      launch_substep<double>(1, a1);
-      for (int st = 2; st <= 4; st++)
-        launch_substep<double>(st, substep_args(g, rt, bt, w, s, dt, st, w->state + 1, tile));
-    }
-    NRPYELL_CUDA(cudaStreamEndCapture(stream(), &graph));
-    g_launches = launches_before;  // captured launches run when the graph does
-    if (!status_ok()) return -1;
-    rg = new RelaxGraph();
-    rg->nodes = 0;
-    NRPYELL_CUDA(cudaGraphGetNodes(graph, nullptr, &rg->nodes));
-    rg->key = *g;
-    rg->dt = dt;
-    rg->tol = log10_tol;
-    rg->R = integration_radius;
-    rg->max_steps = max_steps;
-    rg->scratch_gen = scratch_generation();
-    rg->work_gen = g_work_generation;
-    rg->tile = tile;
-    NRPYELL_CUDA(cudaGraphInstantiate(&rg->exec, graph, 0));
-    NRPYELL_CUDA(cudaGraphDestroy(graph));
-    g_graphs.push_back(rg);
-  }
-
-  static int* pinned = nullptr;
-  static cudaEvent_t ev[2];
-  if (!pinned) {
-    NRPYELL_CUDA(cudaMallocHost(&pinned, sizeof(int) * 16));
-    NRPYELL_CUDA(cudaEventCreateWithFlags(&ev[0], cudaEventDisableTiming));
-    NRPYELL_CUDA(cudaEventCreateWithFlags(&ev[1], cudaEventDisableTiming));
-  }
-  NRPYELL_CUDA(cudaMemsetAsync(w->state, 0, sizeof(int) * 4, stream()));
-  // Replay; poll the state of launch k-1 while launch k runs.
-  const long long max_launches = (long long)max_steps / kStepsPerGraph + 2;
-  for (long long k = 0; k < max_launches; k++) {
-    NRPYELL_CUDA(cudaGraphLaunch(rg->exec, stream()));
-    count_launch((int)rg->nodes);
-    const int slot = (int)(k & 1);
-    NRPYELL_CUDA(cudaMemcpyAsync(pinned + 4 * slot, w->state, sizeof(int) * 4, cudaMemcpyDeviceToHost, stream()));
-    NRPYELL_CUDA(cudaEventRecord(ev[slot], stream()));
-    if (k > 0) {
-      NRPYELL_CUDA(cudaEventSynchronize(ev[1 - slot]));
-      if (pinned[4 * (1 - slot) + 1]) break;
-    }
-    if (!status_ok()) return -1;
-  }
-  // ghost zones of the solution, as the reference's all-points update leaves them
-  launch_ghost_fill<double>(d, bt, g->gridfuncs.y_n_gfs);
+  const Dims d = su.d;
+  const long long n2 = 2 * d.Ntot;
+  FusedWork* w = su.w;
+  if (!w->f32) NRPYELL_CUDA(cudaMalloc(&w->f32, sizeof(float) * (4 * n2 + 3 * d.Ntot)));
+  if (!status_ok()) return -1;
+  StateBuffers b32;
+  b32.y = w->f32;
+  b32.acc = w->f32 + n2;
+  b32.kodd = w->f32 + 2 * n2;
+  b32.keven = w->f32 + 3 * n2;
+  b32.aux = w->f32 + 4 * n2;
+  const StateBuffers b64 = buffers_of(&g->gridfuncs);
+  // Phase 1: FP32 storage and arithmetic (residual norm accumulated in FP64)
+  // until log10 L2 <= log10_switch or the residual stalls.
+  convert_to_float(g->gridfuncs.auxevol_gfs, (float*)b32.aux, 3 * d.Ntot);
+  convert_to_float(g->gridfuncs.y_n_gfs, (float*)b32.y, n2);
+  RelaxParams rp = relax_params(&g->params, dt);
+  rp.log10_tol = log10_switch;
+  rp.max_steps = max_steps;
+  rp.stall_window = stall_window;
+  rp.stall_log_drop = log10(stall_factor);
+  const int tile32 = tuned_tile<float>(d, su.rt, su.bt, w, su.s, b32, rp);
+  const RelaxResult r32 = relax_loop<float>(d, su.rt, su.bt, su.lt, w, su.s, tile32, b32, rp);
+  if (!status_ok()) return -1;
+  // Phase 2: FP64 from the FP32 state to the final tolerance.
+  convert_to_double((const float*)b32.y, g->gridfuncs.y_n_gfs, n2);
+  RelaxParams rp64 = relax_params(&g->params, dt);
+  rp64.log10_tol = log10_tol;
+  rp64.max_steps = max_steps - r32.steps;
+  rp64.history_offset = r32.steps;
+  const int tile64 = tuned_tile<double>(d, su.rt, su.bt, w, su.s, b64, rp64);
+  const RelaxResult r64 = relax_loop<double>(d, su.rt, su.bt, su.lt, w, su.s, tile64, b64, rp64);
+  launch_ghost_fill<double>(d, su.bt, g->gridfuncs.y_n_gfs);
+  if (history)
+    NRPYELL_CUDA(cudaMemcpyAsync(history, w->history, sizeof(double) * (r32.steps + r64.steps + 1),
+                                 cudaMemcpyDeviceToHost, stream()));
   NRPYELL_CUDA(cudaStreamSynchronize(stream()));
-  int st[4];
-  NRPYELL_CUDA(cudaMemcpy(st, w->state, sizeof(st), cudaMemcpyDeviceToHost));
   if (!status_ok()) return -1;
-  const int n = st[0];
-  double last = NAN;
-  NRPYELL_CUDA(cudaMemcpy(&last, w->history + n, sizeof(double), cudaMemcpyDeviceToHost));
-  if (history) NRPYELL_CUDA(cudaMemcpy(history, w->history, sizeof(double) * (n + 1), cudaMemcpyDeviceToHost));
-  if (steps_taken) *steps_taken = n;
-  if (final_log10_l2) *final_log10_l2 = last;
-  if (!status_ok()) return -1;
-  return st[2] ? 0 : 1;
+  if (steps_fp32) *steps_fp32 = r32.steps;
+  if (steps_fp64) *steps_fp64 = r64.steps;
+  if (final_log10_l2) *final_log10_l2 = r64.last_log10_l2;
+  return r64.converged ? 0 : 1;
 }
 
 int nrpyell_relax_host(const paramstruct* params, REAL* xx[3], const bc_struct* bcstruct, const rfm_struct* rfmstruct,
@@ -707,8 +565,7 @@ int nrpyell_relax_host(const paramstruct* params, REAL* xx[3], const bc_struct* 
                        const int max_steps, const REAL integration_radius, int* steps_taken, REAL* final_log10_l2) {
   static griddata_struct g;
   static size_t have = 0;
-  const size_t ntot =
-      (size_t)params->Nxx_plus_2NGHOSTS0 * params->Nxx_plus_2NGHOSTS1 * params->Nxx_plus_2NGHOSTS2;
+  const size_t ntot = (size_t)params->Nxx_plus_2NGHOSTS0 * params->Nxx_plus_2NGHOSTS1 * params->Nxx_plus_2NGHOSTS2;
   if (have != ntot) {
     if (have) {
       NRPYELL_CUDA(cudaStreamSynchronize(stream()));

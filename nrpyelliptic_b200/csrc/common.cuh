@@ -18,6 +18,8 @@ cudaStream_t stream();
 // never creates one.
 cudaStream_t existing_stream();
 void count_launch(int n = 1);
+long long launch_count();
+void set_launch_count(long long n);
 
 #define NRPYELL_CUDA(call)                                                     \
   do {                                                                         \

@@ -41,6 +41,12 @@ struct SubstepArgs {
   double* history;
   double log10_tol;
   int max_steps;
+  // Optional stall test: stop (state[3] = 1) once the best log10 L2 so far
+  // has not dropped by at least -stall_log_drop for stall_window steps;
+  // stall[0..1] = best log10 L2 and the step it was reached.
+  double* stall;
+  int stall_window;
+  double stall_log_drop;
   const int* done;  // kernels return at entry when *done != 0
   int tile;         // tile shape index (autotuned)
 };

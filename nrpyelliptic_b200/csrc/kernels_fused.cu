@@ -51,6 +51,9 @@ struct SubDev {
   const int* done;
   double volume, log10_tol;
   int max_steps;
+  double* stall;
+  int stall_window;
+  double stall_log_drop;
   T dt, eta;
   T cOB[2];
   double invdx0, invdx1;
@@ -233,8 +236,25 @@ __global__ void __launch_bounds__(32 * BY) k_substep(SubDev<T> a) {
           const double l2 = log10(1e-16 + sqrt(tot / a.volume));
           const int n = a.state[0];
           if (a.history) a.history[n] = l2;
+          // Stall test on the best residual so far: the relaxation residual
+          // oscillates (and grows for a while after a cold start), so only a
+          // lack of progress of the running minimum over a whole window
+          // counts, and only once that minimum is within two decades of the
+          // tolerance of this phase -- a precision floor shows up there.
+          bool stalled = false;
+          if (a.stall_window > 0) {
+            if (n == 0 || l2 < a.stall[0] + a.stall_log_drop) {
+              a.stall[0] = l2;
+              a.stall[1] = (double)n;
+            } else if (n - (int)a.stall[1] >= a.stall_window && a.stall[0] <= a.log10_tol + 2.0) {
+              stalled = true;
+            }
+          }
           if (l2 <= a.log10_tol) {
             a.state[2] = 1;
+            a.state[1] = 1;
+          } else if (stalled) {
+            a.state[3] = 1;
             a.state[1] = 1;
           } else if (n >= a.max_steps) {
             a.state[1] = 1;
@@ -413,6 +433,9 @@ static SubDev<T> make_dev(const SubstepArgs& a) {
   f.volume = a.lt ? a.lt->volume : 1.0;
   f.log10_tol = a.log10_tol;
   f.max_steps = a.max_steps;
+  f.stall = a.stall;
+  f.stall_window = a.stall_window;
+  f.stall_log_drop = a.stall_log_drop;
   f.dt = (T)a.dt;
   f.eta = (T)a.eta;
   f.cOB[0] = (T)a.cOB[0];
