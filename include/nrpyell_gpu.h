@@ -125,9 +125,18 @@ void nrpyell_set_async(int enable);
  * every shape on the caller's grid the first time a grid size is stepped
  * and keeps the fastest.  nrpyell_set_tile(t) forces shape t (-1: autotune);
  * nrpyell_get_tile reports the shape in use for a grid (block 32 x by threads,
- * `planes` consecutive i2 planes per thread), -1 if not tuned yet. */
+ * `planes` consecutive i2 planes per thread), -1 if not tuned yet.
+ * nrpyell_num_tiles gives the number of shapes; nrpyell_tile_info describes
+ * shape t and returns -1 for an index out of range.  kind: 0 one thread per
+ * (i0,i1) column of `planes` points reading its stencil through L1; 2 the
+ * same with the pointwise inputs loaded before the first store; 3 TMA
+ * pipeline (persistent CTAs, tiles staged by tensor-map bulk copies, FP64
+ * only -- FP32 runs shape kind 2 instead); 4 the block's uu planes staged in
+ * shared memory. */
 void nrpyell_set_tile(int tile);
 int nrpyell_get_tile(const paramstruct *params, int fp32, int *bx, int *by, int *planes);
+int nrpyell_num_tiles(void);
+int nrpyell_tile_info(int tile, int *by, int *planes, int *kind);
 /* Selects the CUDA device used by every later call (default: device 0).
  * Call before any other GPU work in the process. */
 int nrpyell_set_device(int device);

@@ -18,7 +18,9 @@ CSRC = os.path.join(HERE, "csrc")
 INCLUDE = os.path.join(ROOT, "include")
 LIB = os.path.join(HERE, "libnrpyell_gpu.so")
 
-SOURCES = ["capi.cu", "driver.cu", "tables.cu", "kernels_ref.cu", "kernels_fused.cu", "noalloc.cu", "setup.cpp"]
+SOURCES = ["capi.cu", "driver.cu", "tables.cu", "kernels_ref.cu", "kernels_fused.cu", "kernels_bulk.cu", "noalloc.cu",
+           "setup.cpp"]
+OBJDIR = os.path.join(HERE, "_build")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 
 
@@ -37,18 +39,28 @@ def _stale(target, deps):
 
 
 def build(force=False, verbose=False):
+    """Compile every source to an object (in parallel) and link the library."""
     srcs = [os.path.join(CSRC, s) for s in SOURCES]
-    deps = srcs + [os.path.join(CSRC, f) for f in os.listdir(CSRC) if f.endswith((".h", ".cuh"))]
-    deps += [os.path.join(INCLUDE, f) for f in os.listdir(INCLUDE) if f.endswith(".h")]
-    if not force and not _stale(LIB, deps):
+    headers = [os.path.join(CSRC, f) for f in os.listdir(CSRC) if f.endswith((".h", ".cuh"))]
+    headers += [os.path.join(INCLUDE, f) for f in os.listdir(INCLUDE) if f.endswith(".h")]
+    if not force and not _stale(LIB, srcs + headers):
         return LIB
-    cmd = [nvcc()] + ARCH + [
-        "-O3", "-lineinfo", "-std=c++17", "-shared",
-        "-Xcompiler", "-fPIC,-fopenmp,-O3",
-        "-Xlinker", "-Bsymbolic",
-        "-I", INCLUDE, "-I", CSRC,
-        "-o", LIB,
-    ] + srcs + ["-lgomp", "-lcudart"]
+    os.makedirs(OBJDIR, exist_ok=True)
+    flags = ARCH + ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC,-fopenmp,-O3", "-I", INCLUDE, "-I", CSRC]
+    jobs = []
+    for src in srcs:
+        obj = os.path.join(OBJDIR, os.path.basename(src) + ".o")
+        if force or _stale(obj, [src] + headers):
+            jobs.append([nvcc()] + flags + ["-c", src, "-o", obj])
+    if verbose:
+        for j in jobs:
+            print(" ".join(j))
+    procs = [subprocess.Popen(j) for j in jobs]
+    failed = [j for j, p in zip(jobs, procs) if p.wait() != 0]
+    if failed:
+        raise subprocess.CalledProcessError(1, failed[0])
+    objs = [os.path.join(OBJDIR, os.path.basename(s) + ".o") for s in srcs]
+    cmd = [nvcc()] + ARCH + ["-shared", "-Xlinker", "-Bsymbolic", "-o", LIB] + objs + ["-lgomp", "-lcudart"]
     if verbose:
         print(" ".join(cmd))
     subprocess.run(cmd, check=True)

@@ -49,6 +49,18 @@ cudaStream_t stream() {
 
 cudaStream_t existing_stream() { return g_stream; }
 
+static cudaStream_t g_side_stream = nullptr;
+cudaStream_t side_stream() {
+  if (!g_side_stream) {
+    cudaError_t e = cudaStreamCreateWithFlags(&g_side_stream, cudaStreamNonBlocking);
+    if (e != cudaSuccess) {
+      g_side_stream = nullptr;
+      report_error(__FILE__, __LINE__, cudaGetErrorString(e));
+    }
+  }
+  return g_side_stream;
+}
+
 void count_launch(int n) { g_launches += n; }
 long long launch_count() { return g_launches; }
 void set_launch_count(long long n) { g_launches = n; }
@@ -232,6 +244,18 @@ int nrpyell_get_tile(const paramstruct* params, int fp32, int* bx, int* by, int*
   int tile = g_forced_tile >= 0 ? g_forced_tile : find_tile(dims_of(params), fp32);
   if (tile >= 0 && bx && by && planes) substep_tile_shape(tile, bx, by, planes);
   return tile;
+}
+
+int nrpyell_num_tiles(void) { return substep_num_tiles(); }
+
+int nrpyell_tile_info(int tile, int* by, int* planes, int* kind) {
+  if (tile < 0 || tile >= substep_num_tiles()) return -1;
+  int bx = 0, b = 0, p = 0;
+  substep_tile_shape(tile, &bx, &b, &p);
+  if (by) *by = b;
+  if (planes) *planes = p;
+  if (kind) *kind = substep_tile_kind(tile);
+  return 0;
 }
 
 int nrpyell_set_device(int device) {

@@ -17,6 +17,9 @@ cudaStream_t stream();
 // The library's stream if it has been created, else the default stream (0);
 // never creates one.
 cudaStream_t existing_stream();
+// Second stream of the library, created on first use: work that may overlap
+// a kernel of stream() (forked from and joined back into stream()).
+cudaStream_t side_stream();
 void count_launch(int n = 1);
 long long launch_count();
 void set_launch_count(long long n);
@@ -38,6 +41,12 @@ void set_launch_count(long long n);
 #define NRPYELL_LAUNCH(kernel, grid, block, smem, ...)                         \
   do {                                                                         \
     kernel<<<(grid), (block), (smem), ::nrpyell::stream()>>>(__VA_ARGS__);     \
+    ::nrpyell::count_launch();                                                 \
+    NRPYELL_CUDA(cudaGetLastError());                                          \
+  } while (0)
+#define NRPYELL_LAUNCH_ON(strm, kernel, grid, block, smem, ...)                \
+  do {                                                                         \
+    kernel<<<(grid), (block), (smem), (strm)>>>(__VA_ARGS__);                  \
     ::nrpyell::count_launch();                                                 \
     NRPYELL_CUDA(cudaGetLastError());                                          \
   } while (0)

@@ -48,6 +48,7 @@ struct SubstepArgs {
   int stall_window;
   double stall_log_drop;
   const int* done;  // kernels return at entry when *done != 0
+  int* err;         // a kernel whose bounded wait gave up stores a nonzero code
   int tile;         // tile shape index (autotuned)
 };
 template <typename T>
@@ -55,8 +56,29 @@ void launch_substep(int stage, const SubstepArgs& a);
 // Copies inner ghost points of gfs (2 gridfunctions) from their sources.
 template <typename T>
 void launch_ghost_fill(const Dims& d, const BcTables* bt, void* gfs);
+// Tile shapes: 32 x by x p points per interior tile, of the kinds listed at
+// nrpyell_tile_info.
 int substep_num_tiles();
 void substep_tile_shape(int tile, int* bx, int* by, int* p);
+int substep_tile_kind(int tile);  // see nrpyell_tile_info
 int substep_interior_blocks(const Dims& d, int tile);
+// One-time per-shape setup (shared-memory opt-in); call before a stream
+// capture that launches the shape.
+template <typename T>
+void prepare_substep(int tile);
+
+// Radiation-BC columns of a substep as their own kernel on side_stream(),
+// forked from stream(); join_columns() makes stream() wait for them.
+// prepare_columns() creates the stream and events (before a capture).
+template <typename T>
+void launch_columns_forked(int stage, const SubstepArgs& a);
+void join_columns();
+void prepare_columns();
+
+// ---- bulk-copy pipeline variant (kernels_bulk.cu), FP64 ----
+// Usable when the row length N0 is even and every array is 16-byte aligned.
+bool bulk_available(const SubstepArgs& a, size_t elem_size);
+void launch_bulk(int stage, int shape, const SubstepArgs& a);
+void prepare_bulk(int shape);
 
 }  // namespace nrpyell

@@ -1,4 +1,4 @@
-// Fused RK4 substep kernel: the fast path of MoL_step_forward_in_time and of
+// Fused RK4 substep kernels: the fast path of MoL_step_forward_in_time and of
 // the relaxation drivers.
 //
 // One RK4 substep of the reference (MoL_step_forward_in_time.c:12-176) is
@@ -6,364 +6,348 @@
 // points, the inner-BC copy of the RHS, and a linear combination over every
 // point.  Here the whole substep is ONE kernel launch with two kinds of
 // blocks:
-//   interior blocks: each thread owns an (i0,i1) pair and P consecutive i2
-//     planes; it evaluates the RHS and feeds it straight into the RK
-//     combination (the RHS never touches memory).  Stencil points that fall
-//     in an inner ghost zone are read from their source point (the SymTP
+//   column blocks (first in the launch): the radiation BC of the x0max face,
+//     one (i1,i2) column at a time for both gridfunctions, layers 0..4 inner
+//     to outer (apply_bcs_outerradiation_and_inner.c:369-408), then the RK
+//     combination at those points.  A column recomputes the RHS of its last
+//     interior point itself, so it never waits for an interior block.
+//   interior blocks: the RHS at every interior point straight into the RK
+//     combination (the RHS never touches memory).  Stencil points in an
+//     inner ghost zone are read from their source point (the SymTP
 //     reflections of symtp_ghost_source, verified against the caller's
 //     bc_struct), so inner ghost zones are never written or read during a
 //     relaxation.  At stage 1 the residual -- the vv-RHS bracket before the
-//     wavespeed^2 factor -- is squared, weighted and reduced per block; the
-//     last block to finish forms the L2 norm in a fixed order and runs the
+//     wavespeed^2 factor -- is squared, weighted, reduced per tile, and the
+//     last tile to finish forms the L2 norm in a fixed order and runs the
 //     stop test.
-//   column blocks: the radiation BC of the x0max face, one (i1,i2) column at
-//     a time for both gridfunctions, layers g = 0..4 inner to outer
-//     (apply_bcs_outerradiation_and_inner.c:369-408), followed by the RK
-//     combination at those points.  A column recomputes the RHS of its last
-//     interior point itself, so it never waits for an interior block.
+// This file holds the direct variant: each thread owns an (i0,i1) pair and P
+// consecutive i2 planes, holds uu along i2 in registers and reads the rest of
+// its 31-point star through L1 (optionally loading the pointwise inputs of
+// all P planes before the first store).  kernels_bulk.cu holds the
+// bulk-copy pipeline variant; the autotuner picks among the shapes of both.
 // The metric factors of the RHS depend on (i0,i1) only and are folded into
 // six per-(i0,i1) weights (tables.cu), leaving one division per point.
-#include "fd_weights.h"
-#include "kernels.cuh"
+#include "substep.cuh"
 
 namespace nrpyell {
 
-__constant__ double c_fd1w[11][11] = NRPYELL_FD1_UPWIND_INIT;
-
-template <typename T>
-struct SubDev {
-  int N0, N1, Nxx0, Nxx1, Nxx2, half2;
-  long long N01, Ntot;
-  int tiles0, tiles1, tiles2;  // interior tile grid
-  int n_int_blocks, ncol, n_col_blocks;
-  const T* __restrict__ S;     // stage input
-  const T* y;                  // y_n (aliases out at stage 4)
-  T* acc;
-  T* out;
-  const T* __restrict__ aux;
-  const T* __restrict__ coef;
-  const double* __restrict__ colgeo;
-  const double* __restrict__ w;  // L2 weights (stage-1 residual)
-  double* partials;
-  unsigned int* ticket;
-  int* state;  // [0] n, [1] done, [2] converged
-  double* history;
-  const int* done;
-  double volume, log10_tol;
-  int max_steps;
-  double* stall;
-  int stall_window;
-  double stall_log_drop;
-  T dt, eta;
-  T cOB[2];
-  double invdx0, invdx1;
-};
-
-// Interior index along i2 after a wrap by 2 pi.
-__device__ __forceinline__ int wrap2(int j, int Nxx2) {
-  j -= NGHOSTS;
-  if (j < 0) j += Nxx2;
-  if (j >= Nxx2) j -= Nxx2;
-  return j + NGHOSTS;
-}
-
-template <typename T, int STAGE>
-__device__ __forceinline__ void rk_combine(T k, T yv, T& acc, T& out, T dt) {
-  const T dk = dt * k;
-  if (STAGE == 1) {
-    acc = (T)(1.0 / 6.0) * dk;
-    out = fma((T)0.5, dk, yv);
-  } else if (STAGE == 2) {
-    acc = fma((T)(1.0 / 3.0), dk, acc);
-    out = fma((T)0.5, dk, yv);
-  } else if (STAGE == 3) {
-    acc = fma((T)(1.0 / 3.0), dk, acc);
-    out = fma(dt, k, yv);
-  } else {
-    out = yv + fma((T)(1.0 / 6.0), dk, acc);
-  }
-}
-
-// RHS of (uu, vv) at one interior point from the raw stencil sums.  Shared by
-// interior threads and column blocks so both produce identical bits.
-template <typename T>
-__device__ __forceinline__ void point_rhs(const SubDev<T>& a, long long idx, int k2, T c, T s0, T s1, T s00, T s11,
-                                          T s22, T& ku, T& kv, T& bracket) {
-  const long long n01 = a.N01;
-  const T C22 = __ldg(a.coef + k2), C00 = __ldg(a.coef + n01 + k2), C11 = __ldg(a.coef + 2 * n01 + k2);
-  const T C1 = __ldg(a.coef + 3 * n01 + k2), C0 = __ldg(a.coef + 4 * n01 + k2), Cc = __ldg(a.coef + 5 * n01 + k2);
-  const T AA = __ldg(a.aux + ADD_TIMES_AUUGF * a.Ntot + idx);
-  const T psi = __ldg(a.aux + PSI_BACKGROUNDGF * a.Ntot + idx);
-  const T ws = __ldg(a.aux + WAVESPEEDGF * a.Ntot + idx);
-  const T vv = __ldg(a.S + a.Ntot + idx);
-  const T pu = psi + c;
-  const T pu2 = pu * pu;
-  const T pu4 = pu2 * pu2;
-  const T pu7 = pu4 * pu2 * pu;
-  T lap = Cc * c;
-  lap = fma(C00, s00, lap);
-  lap = fma(C11, s11, lap);
-  lap = fma(C22, s22, lap);
-  lap = fma(C1, s1, lap);
-  lap = fma(C0, s0, lap);
-  bracket = fma((T)0.125, AA / pu7, lap);
-  ku = fma(-a.eta, c, vv);
-  kv = (ws * ws) * bracket;
-}
-
-// 10th-order weights (rhs_eval.c:23-27): first derivative d_k, second e_k.
-template <typename T>
-struct W {
-  static __device__ __forceinline__ T d(int k) {
-    return k == 1 ? (T)(5.0 / 6.0) : k == 2 ? (T)(-5.0 / 21.0) : k == 3 ? (T)(5.0 / 84.0) : k == 4 ? (T)(-5.0 / 504.0) : (T)(1.0 / 1260.0);
-  }
-  static __device__ __forceinline__ T e(int k) {
-    return k == 1 ? (T)(5.0 / 3.0) : k == 2 ? (T)(-5.0 / 21.0) : k == 3 ? (T)(5.0 / 126.0) : k == 4 ? (T)(-5.0 / 1008.0) : (T)(1.0 / 3150.0);
-  }
-};
-
-// Stencil sums along i0 and i1 at interior point (i0,i1,i2); ghost neighbours
-// are read from their source points.  i2h is the i2 index shifted by pi.
-template <typename T>
-__device__ __forceinline__ void stencil01(const SubDev<T>& a, const T* __restrict__ u, int i0, int i1, int i2, int i2h,
-                                          T& s0, T& s1, T& s00, T& s11) {
-  const long long base = i0 + (long long)a.N0 * i1 + a.N01 * i2;
-  const long long rowh = (long long)a.N0 * i1 + a.N01 * i2h;  // (.,i1,i2h)
-  const long long colh = i0 + a.N01 * i2h;                     // (i0,.,i2h)
-  const int top = NGHOSTS + a.Nxx1;
-#pragma unroll
-  for (int k = 1; k <= 5; k++) {
-    const int j0 = i0 - k;
-    const long long im = (j0 >= NGHOSTS) ? base - k : (2 * NGHOSTS - 1 - j0) + rowh;
-    const int jm = i1 - k, jp = i1 + k;
-    const long long jmi = (jm >= NGHOSTS) ? base - (long long)k * a.N0 : colh + (long long)a.N0 * (2 * NGHOSTS - 1 - jm);
-    const long long jpi = (jp < top) ? base + (long long)k * a.N0 : colh + (long long)a.N0 * (2 * top - 1 - jp);
-    const T am = __ldg(u + im), ap = __ldg(u + base + k);
-    const T bm = __ldg(u + jmi), bp = __ldg(u + jpi);
-    s0 = fma(W<T>::d(k), ap - am, s0);
-    s1 = fma(W<T>::d(k), bp - bm, s1);
-    s00 = fma(W<T>::e(k), ap + am, s00);
-    s11 = fma(W<T>::e(k), bp + bm, s11);
-  }
-}
-
-constexpr int kColThreadsPerColumn = 16;
-
-template <typename T, int STAGE, bool RESID, int BY, int P>
+// ------------------------------------------------------- direct interior
+template <typename T, int STAGE, bool RESID, int BY, int P, bool PF>
 __global__ void __launch_bounds__(32 * BY) k_substep(SubDev<T> a) {
   constexpr int NT = 32 * BY;
-  constexpr int CB = NT / kColThreadsPerColumn;
   __shared__ double sh[NT / 32 > 8 ? NT / 32 : 8];
-  __shared__ bool last_block;
-  __shared__ double drf[CB][2][6], fvs[CB][2][6], kl[CB][2], kk[CB][2][5];
+  __shared__ bool last;
   if (*a.done) return;
-  const int tid = threadIdx.x;
-  // Column blocks come first in the launch order: their dependent load
-  // chains then overlap with the interior blocks instead of forming a tail.
-  if ((int)blockIdx.x >= a.n_col_blocks) {
-    // ------------------------------------------------------------ interior
-    const int b = blockIdx.x - a.n_col_blocks;
-    const int t0 = b % a.tiles0, t1 = (b / a.tiles0) % a.tiles1, t2 = b / (a.tiles0 * a.tiles1);
-    const int i0 = t0 * 32 + (tid & 31) + NGHOSTS;
-    const int i1 = t1 * BY + (tid >> 5) + NGHOSTS;
-    const int z0 = t2 * P + NGHOSTS;
-    double r2 = 0.0;
-    if (i0 < NGHOSTS + a.Nxx0 && i1 < NGHOSTS + a.Nxx1) {
-      const T* u = a.S;
-      const long long line = i0 + (long long)a.N0 * i1;
-      // uu along i2 for planes z0-5 .. z0+P+4 (wrapped by 2 pi)
-      T col[P + 10];
-#pragma unroll
-      for (int q = 0; q < P + 10; q++) col[q] = __ldg(u + line + a.N01 * wrap2(z0 - 5 + q, a.Nxx2));
-      const int k2 = i0 + a.N0 * i1;
-#pragma unroll
-      for (int p = 0; p < P; p++) {
-        const int i2 = z0 + p;
-        if (i2 < NGHOSTS + a.Nxx2) {
-          const int i2h = wrap2(i2 + a.half2, a.Nxx2);
-          T s0 = 0, s1 = 0, s00 = 0, s11 = 0, s22 = 0;
-          stencil01<T>(a, u, i0, i1, i2, i2h, s0, s1, s00, s11);
-#pragma unroll
-          for (int k = 1; k <= 5; k++) s22 = fma(W<T>::e(k), col[p + 5 + k] + col[p + 5 - k], s22);
-          const long long idx = line + a.N01 * i2;
-          T ku, kv, br;
-          point_rhs<T>(a, idx, k2, col[p + 5], s0, s1, s00, s11, s22, ku, kv, br);
-          T accu = (STAGE == 1) ? (T)0 : a.acc[idx];
-          T accv = (STAGE == 1) ? (T)0 : a.acc[a.Ntot + idx];
-          const T yu = a.y[idx], yv = a.y[a.Ntot + idx];
-          T ou, ov;
-          rk_combine<T, STAGE>(ku, yu, accu, ou, a.dt);
-          rk_combine<T, STAGE>(kv, yv, accv, ov, a.dt);
-          if (STAGE != 4) {
-            a.acc[idx] = accu;
-            a.acc[a.Ntot + idx] = accv;
-          }
-          a.out[idx] = ou;
-          a.out[a.Ntot + idx] = ov;
-          if (RESID) {
-            const double bb = (double)br;
-            r2 += bb * bb * __ldg(a.w + k2);
-          }
-        }
-      }
-    }
-    if (RESID) {
-      // per-block partial in a fixed order, then the last block forms the norm
-#pragma unroll
-      for (int o = 16; o > 0; o >>= 1) r2 += __shfl_down_sync(0xffffffffu, r2, o);
-      if ((tid & 31) == 0) sh[tid >> 5] = r2;
-      __syncthreads();
-      if (tid == 0) {
-        double t = 0.0;
-        for (int wi = 0; wi < NT / 32; wi++) t += sh[wi];
-        a.partials[b] = t;
-        __threadfence();
-        last_block = (atomicAdd(a.ticket, 1u) == (unsigned)a.n_int_blocks - 1);
-      }
-      __syncthreads();
-      if (last_block) {
-        __threadfence();
-        double v = 0.0;
-        for (int i = tid; i < a.n_int_blocks; i += NT) v += ((volatile double*)a.partials)[i];
-#pragma unroll
-        for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
-        __syncthreads();
-        if ((tid & 31) == 0) sh[tid >> 5] = v;
-        __syncthreads();
-        if (tid == 0) {
-          double tot = 0.0;
-          for (int wi = 0; wi < NT / 32; wi++) tot += sh[wi];
-          const double l2 = log10(1e-16 + sqrt(tot / a.volume));
-          const int n = a.state[0];
-          if (a.history) a.history[n] = l2;
-          // Stall test on the best residual so far: the relaxation residual
-          // oscillates (and grows for a while after a cold start), so only a
-          // lack of progress of the running minimum over a whole window
-          // counts, and only once that minimum is within two decades of the
-          // tolerance of this phase -- a precision floor shows up there.
-          bool stalled = false;
-          if (a.stall_window > 0) {
-            if (n == 0 || l2 < a.stall[0] + a.stall_log_drop) {
-              a.stall[0] = l2;
-              a.stall[1] = (double)n;
-            } else if (n - (int)a.stall[1] >= a.stall_window && a.stall[0] <= a.log10_tol + 2.0) {
-              stalled = true;
-            }
-          }
-          if (l2 <= a.log10_tol) {
-            a.state[2] = 1;
-            a.state[1] = 1;
-          } else if (stalled) {
-            a.state[3] = 1;
-            a.state[1] = 1;
-          } else if (n >= a.max_steps) {
-            a.state[1] = 1;
-          } else {
-            a.state[0] = n + 1;
-          }
-          *a.ticket = 0u;
-          __threadfence();
-        }
-      }
-    }
+  if ((int)blockIdx.x < a.n_col_blocks) {
+    column_block<T, STAGE, NT>(a, blockIdx.x);
     return;
   }
+  const int tid = threadIdx.x;
+  const int b = blockIdx.x - a.n_col_blocks;
+  const int t0 = b % a.tiles0, t1 = (b / a.tiles0) % a.tiles1, t2 = b / (a.tiles0 * a.tiles1);
+  const int i0 = t0 * 32 + (tid & 31) + NGHOSTS;
+  const int i1 = t1 * BY + (tid >> 5) + NGHOSTS;
+  const int z0 = t2 * P + NGHOSTS;
+  double r2 = 0.0;
+  if (i0 < NGHOSTS + a.Nxx0 && i1 < NGHOSTS + a.Nxx1) {
+    const T* u = a.S;
+    const long long line = i0 + (long long)a.N0 * i1;
+    const long long Ntot = a.Ntot;
+    // uu along i2 for planes z0-5 .. z0+P+4 (wrapped by 2 pi)
+    T col[P + 10];
+#pragma unroll
+    for (int q = 0; q < P + 10; q++) col[q] = __ldg(u + line + a.N01 * wrap2(z0 - 5 + q, a.Nxx2));
+    // PF: every pointwise input of the P planes is loaded before the first
+    // store (the stores may alias y_n, so the compiler cannot hoist them).
+    T pf[8][P];  // unused (and removed) when !PF
+    if (PF) {
+#pragma unroll
+      for (int p = 0; p < P; p++) {
+        const long long idx = line + a.N01 * (z0 + p < NGHOSTS + a.Nxx2 ? z0 + p : z0);
+        pf[0][p] = __ldg(a.S + Ntot + idx);
+        pf[1][p] = __ldg(a.aux + ADD_TIMES_AUUGF * Ntot + idx);
+        pf[2][p] = __ldg(a.aux + PSI_BACKGROUNDGF * Ntot + idx);
+        pf[3][p] = __ldg(a.aux + WAVESPEEDGF * Ntot + idx);
+        pf[4][p] = a.y[idx];
+        pf[5][p] = a.y[Ntot + idx];
+        pf[6][p] = (STAGE == 1) ? (T)0 : a.acc[idx];
+        pf[7][p] = (STAGE == 1) ? (T)0 : a.acc[Ntot + idx];
+      }
+    }
+    const int k2 = i0 + a.N0 * i1;
+#pragma unroll
+    for (int p = 0; p < P; p++) {
+      const int i2 = z0 + p;
+      if (i2 < NGHOSTS + a.Nxx2) {
+        const int i2h = wrap2(i2 + a.half2, a.Nxx2);
+        T s0 = 0, s1 = 0, s00 = 0, s11 = 0, s22 = 0;
+        stencil01<T>(a, u, i0, i1, i2, i2h, s0, s1, s00, s11);
+#pragma unroll
+        for (int k = 1; k <= 5; k++) s22 = fma(W<T>::e(k), col[p + 5 + k] + col[p + 5 - k], s22);
+        const long long idx = line + a.N01 * i2;
+        T ku, kv, br;
+        if (PF) {
+          const long long n01 = a.N01;
+          point_rhs<T>(col[p + 5], pf[0][p], pf[1][p],
+                       pf[2][p], pf[3][p],
+                       __ldg(a.coef + k2), __ldg(a.coef + n01 + k2), __ldg(a.coef + 2 * n01 + k2),
+                       __ldg(a.coef + 3 * n01 + k2), __ldg(a.coef + 4 * n01 + k2), __ldg(a.coef + 5 * n01 + k2), s0,
+                       s1, s00, s11, s22, a.eta, ku, kv, br);
+          store_point<T, STAGE>(a, idx, ku, kv, pf[4][p],
+                                pf[5][p], pf[6][p],
+                                pf[7][p]);
+        } else {
+          point_rhs_global<T>(a, idx, k2, col[p + 5], s0, s1, s00, s11, s22, ku, kv, br);
+          const T accu = (STAGE == 1) ? (T)0 : a.acc[idx];
+          const T accv = (STAGE == 1) ? (T)0 : a.acc[Ntot + idx];
+          store_point<T, STAGE>(a, idx, ku, kv, a.y[idx], a.y[Ntot + idx], accu, accv);
+        }
+        if (RESID) {
+          const double bb = (double)br;
+          r2 += bb * bb * __ldg(a.w + k2);
+        }
+      }
+    }
+  }
+  if (RESID && tile_partial<NT>(r2, b, a.partials, a.ticket, a.n_tiles, sh, &last)) finalize_l2<T, NT>(a, sh);
+}
 
-  // -------------------------------------------------------------- columns
-  // Column c of this block, task r: r < 12 -> d f/d r at point jj = r % 6 of
-  // gridfunction g = r / 6 (point jj is i0 = N0-6+jj; jj = 0 is the last
-  // interior plane, jj = 1..5 the outer layers 0..4); r == 12 -> RHS at the
-  // last interior point.
-  const int cb = blockIdx.x;
-  const int c = tid / kColThreadsPerColumn, r = tid % kColThreadsPerColumn;
-  const int colid = cb * CB + c;
-  const bool live = colid < a.ncol;
-  const int i1 = NGHOSTS + (live ? colid % a.Nxx1 : 0);
-  const int i2 = NGHOSTS + (live ? colid / a.Nxx1 : 0);
+// ------------------------------------------------ radiation columns by rows
+// The radiation BC of the x0max face: the column blocks of the shared-memory
+// planes kernel, and a kernel of its own that runs beside the persistent TMA
+// pipeline kernel on the side stream.  A block takes
+// kRows consecutive i1 columns at one i2: it copies the outer 12 points of
+// uu and vv along i0 on those rows and on 5 rows either side (rows across
+// the axis from their images) into shared memory, then computes every
+// column's 12 radial derivatives, the RHS of its last interior point, the
+// layer recurrence and the RK combination with the same arithmetic as
+// column_block.
+constexpr int kRows = 32;
+
+// Shared memory of column_rows, in doubles: F[2][kRows+10][12], drf and fvs
+// [kRows][2][6], kl [kRows][2], kk [kRows][2][5].
+constexpr int kRowsSmem = 2 * (kRows + 10) * 12 + 2 * kRows * 12 + kRows * 2 + kRows * 10;
+
+template <typename T, int STAGE, int NT>
+__device__ void column_rows(const SubDev<T>& a, int cb, double* smem) {
+  static_assert(NT >= 2 * kRows, "the layer recurrence takes one thread per column and gridfunction");
+  constexpr int NRW = kRows + 10, NQ = 12;
+  double(*F)[NRW][NQ] = reinterpret_cast<double(*)[NRW][NQ]>(smem);
+  double(*drf)[2][6] = reinterpret_cast<double(*)[2][6]>(smem + 2 * NRW * NQ);
+  double(*fvs)[2][6] = reinterpret_cast<double(*)[2][6]>(smem + 2 * NRW * NQ + kRows * 12);
+  double(*kl)[2] = reinterpret_cast<double(*)[2]>(smem + 2 * NRW * NQ + 2 * kRows * 12);
+  double(*kk)[2][5] = reinterpret_cast<double(*)[2][5]>(smem + 2 * NRW * NQ + 2 * kRows * 12 + 2 * kRows);
+  const int tid = threadIdx.x;
+  const int nb1 = (a.Nxx1 + kRows - 1) / kRows;
+  const int i1a = NGHOSTS + (cb % nb1) * kRows;
+  const int i2 = NGHOSTS + cb / nb1;
+  const int top = NGHOSTS + a.Nxx1;
+  const int ncol = min(kRows, top - i1a);
   const int i2h = wrap2(i2 + a.half2, a.Nxx2);
   const int N0 = a.N0;
-  const long long row = (long long)N0 * i1 + a.N01 * i2;
-  if (live && r < 12) {
-    const int g = r / 6, jj = r % 6;
-    const T* f = a.S + g * a.Ntot;
-    const int ip = N0 - 6 + jj;
-    const int off = (jj <= 1) ? -1 : -jj;  // compute_partial_r_f's upwind offset at i0 = ip
-    const double* wt = c_fd1w[off + 5];
-    double d0 = 0.0;
-#pragma unroll
-    for (int m = 0; m < 11; m++) {
-      const double term = wt[m] * (double)__ldg(f + row + ip + off - 5 + m);
-      d0 = (m == 0) ? term : d0 + term;
+  for (int e = tid; e < 2 * NRW * NQ; e += NT) {
+    const int q = e % NQ, j = (e / NQ) % NRW, g = e / (NQ * NRW);
+    if (j >= ncol + 2 * NGHOSTS) continue;  // not needed
+    int i1 = i1a - NGHOSTS + j, i2s = i2;
+    if (i1 < NGHOSTS) {
+      i1 = 2 * NGHOSTS - 1 - i1;
+      i2s = i2h;
+    } else if (i1 >= top) {
+      i1 = 2 * top - 1 - i1;
+      i2s = i2h;
     }
-    d0 *= a.invdx0;
-    // centred x1 stencil; points across the axis come from their images
-    const int top = NGHOSTS + a.Nxx1;
-    double d1 = 0.0;
-    bool first = true;
-#pragma unroll
-    for (int m = 0; m < 11; m++) {
-      if (m == 5) continue;
-      const int j1 = i1 + m - 5;
-      long long id;
-      if (j1 < NGHOSTS)
-        id = ip + (long long)N0 * (2 * NGHOSTS - 1 - j1) + a.N01 * i2h;
-      else if (j1 >= top)
-        id = ip + (long long)N0 * (2 * top - 1 - j1) + a.N01 * i2h;
-      else
-        id = ip + (long long)N0 * j1 + a.N01 * i2;
-      const double term = c_fd1w[5][m] * (double)__ldg(f + id);
-      d1 = first ? term : d1 + term;
-      first = false;
-    }
-    d1 *= a.invdx1;
-    const double dx0dr = __ldg(a.colgeo + (1 * 6 + jj) * a.N1 + i1);
-    const double dx1dr = __ldg(a.colgeo + (2 * 6 + jj) * a.N1 + i1);
-    drf[c][g][jj] = dx0dr * d0 + dx1dr * d1;
-    fvs[c][g][jj] = (double)__ldg(f + row + ip);
-  } else if (live && r == 12) {
-    const int i0 = N0 - NGHOSTS - 1;
-    const T* u = a.S;
-    const long long idx = row + i0;
-    T s0 = 0, s1 = 0, s00 = 0, s11 = 0, s22 = 0;
-    stencil01<T>(a, u, i0, i1, i2, i2h, s0, s1, s00, s11);
-    const long long line = i0 + (long long)N0 * i1;
-#pragma unroll
-    for (int k = 1; k <= 5; k++)
-      s22 = fma(W<T>::e(k),
-                __ldg(u + line + a.N01 * wrap2(i2 + k, a.Nxx2)) + __ldg(u + line + a.N01 * wrap2(i2 - k, a.Nxx2)), s22);
-    T ku, kv, br;
-    point_rhs<T>(a, idx, i0 + N0 * i1, __ldg(u + idx), s0, s1, s00, s11, s22, ku, kv, br);
-    kl[c][0] = (double)ku;
-    kl[c][1] = (double)kv;
+    F[g][j][q] = (double)__ldg(a.S + g * a.Ntot + (N0 - NQ + q) + (long long)N0 * i1 + a.N01 * i2s);
   }
   __syncthreads();
-  if (live && r < 2) {
-    const int g = r;
-    const double cw = (double)a.cOB[g];
-    double kprev = kl[c][g];
+  // radial derivatives at the last interior point and the 5 layers (items
+  // c*12 + g*6 + jj), then the RHS of each column's last interior point
+  for (int it = tid; it < kRows * 13; it += NT) {
+    if (it < kRows * 12) {
+      const int c = it / 12, g = (it / 6) % 2, jj = it % 6;
+      if (c >= ncol) continue;
+      const int off = (jj <= 1) ? -1 : -jj;
+      double v[11];
 #pragma unroll
-    for (int L = 0; L < NGHOSTS; L++) {
-      const double rn = __ldg(a.colgeo + (0 * 6 + L) * a.N1 + i1);
-      const double rr = __ldg(a.colgeo + (0 * 6 + L + 1) * a.N1 + i1);
-      const double out_int = -cw * (drf[c][g][L] + fvs[c][g][L] / rn);
-      const double K = rn * rn * rn * (kprev - out_int);
-      const double rinv = 1.0 / rr;
-      const double outw = -cw * (drf[c][g][L + 1] + fvs[c][g][L + 1] * rinv);
-      const double k = outw + K * rinv * rinv * rinv;
-      kk[c][g][L] = k;
-      kprev = k;
+      for (int m = 0; m < 11; m++) v[m] = F[g][c + NGHOSTS][1 + jj + off + m];
+      const double d0 = radiation_sum_x0(c_fd1w[off + 5], v);
+#pragma unroll
+      for (int m = 0; m < 11; m++) v[m] = (m == 5) ? 0.0 : F[g][c + m][6 + jj];
+      const double d1 = radiation_sum_x1(v);
+      const int i1 = i1a + c;
+      drf[c][g][jj] = radiation_drf(d0, d1, a.invdx0, a.invdx1, __ldg(a.colgeo + (1 * 6 + jj) * a.N1 + i1),
+                                    __ldg(a.colgeo + (2 * 6 + jj) * a.N1 + i1));
+      fvs[c][g][jj] = F[g][c + NGHOSTS][6 + jj];
+    } else {
+      const int c = it - kRows * 12;
+      if (c >= ncol) continue;
+      const int i1 = i1a + c, i0 = N0 - NGHOSTS - 1;
+      const double* row = F[0][c + NGHOSTS];
+      T s0 = 0, s1 = 0, s00 = 0, s11 = 0, s22 = 0;
+#pragma unroll
+      for (int k = 1; k <= 5; k++) {
+        const T am = (T)row[6 - k], ap = (T)row[6 + k];
+        const T bm = (T)F[0][c + NGHOSTS - k][6], bp = (T)F[0][c + NGHOSTS + k][6];
+        s0 = fma(W<T>::d(k), ap - am, s0);
+        s1 = fma(W<T>::d(k), bp - bm, s1);
+        s00 = fma(W<T>::e(k), ap + am, s00);
+        s11 = fma(W<T>::e(k), bp + bm, s11);
+      }
+      const T* u = a.S;
+      const long long line = i0 + (long long)N0 * i1;
+#pragma unroll
+      for (int k = 1; k <= 5; k++)
+        s22 = fma(W<T>::e(k),
+                  __ldg(u + line + a.N01 * wrap2(i2 + k, a.Nxx2)) + __ldg(u + line + a.N01 * wrap2(i2 - k, a.Nxx2)),
+                  s22);
+      T ku, kv, br;
+      point_rhs_global<T>(a, line + a.N01 * i2, i0 + N0 * i1, (T)row[6], s0, s1, s00, s11, s22, ku, kv, br);
+      kl[c][0] = (double)ku;
+      kl[c][1] = (double)kv;
     }
   }
   __syncthreads();
-  if (live && r < 10) {
-    const int g = r / 5, L = r % 5;
-    const long long idx = g * a.Ntot + row + N0 - NGHOSTS + L;
+  if (tid < 2 * ncol) {
+    const int c = tid / 2, g = tid % 2;
+    radiation_layers((double)a.cOB[g], kl[c][g], drf[c][g], fvs[c][g], a.colgeo + i1a + c, a.N1, kk[c][g]);
+  }
+  __syncthreads();
+  for (int it = tid; it < ncol * 10; it += NT) {
+    const int c = it / 10, g = (it / 5) % 2, L = it % 5;
+    const long long idx = g * a.Ntot + (long long)N0 * (i1a + c) + a.N01 * i2 + N0 - NGHOSTS + L;
     T accv = (STAGE == 1) ? (T)0 : a.acc[idx];
     T ov;
     rk_combine<T, STAGE>((T)kk[c][g][L], a.y[idx], accv, ov, a.dt);
     if (STAGE != 4) a.acc[idx] = accv;
     a.out[idx] = ov;
   }
+}
+
+template <typename T, int STAGE>
+__global__ void __launch_bounds__(128) k_radiation_rows(SubDev<T> a) {
+  __shared__ double smem[kRowsSmem];
+  if (*a.done) return;
+  column_rows<T, STAGE, 128>(a, blockIdx.x, smem);
+}
+
+// ------------------------------------------------- planes in shared memory
+// Same per-point arithmetic as k_substep, but the block first copies uu on
+// its P planes, widened by 5 points along i0 and i1, into shared memory (one
+// warp per row; ghost points redirected to their sources only in blocks that
+// touch an inner boundary), so the i0 and i1 stencil arms are shared-memory
+// reads at compile-time offsets and the per-point integer work is small.
+// uu along i2 stays in registers and the pointwise inputs of all P planes are
+// loaded before the first store.
+template <typename T, int STAGE, bool RESID, int BY, int P>
+__global__ void __launch_bounds__(32 * BY) k_substep_planes(SubDev<T> a) {
+  constexpr int NT = 32 * BY;
+  constexpr int RWS = 42;       // i0 = i00-5 .. i00+36
+  constexpr int NR = BY + 10;   // i1 = i10-5 .. i10+BY+4
+  constexpr int PLANES = (P * NR * RWS * (int)sizeof(T) + 7) / 8;
+  // the planes of an interior block, or the rows of a column block
+  __shared__ double smem[PLANES > kRowsSmem ? PLANES : kRowsSmem];
+  T(*su)[NR][RWS] = reinterpret_cast<T(*)[NR][RWS]>(smem);
+  __shared__ double sh[NT / 32 > 8 ? NT / 32 : 8];
+  __shared__ bool last;
+  if (*a.done) return;
+  if ((int)blockIdx.x < a.n_col_blocks) {
+    column_rows<T, STAGE, NT>(a, blockIdx.x, smem);
+    return;
+  }
+  const int tid = threadIdx.x, tx = tid & 31, ty = tid >> 5;
+  const int b = blockIdx.x - a.n_col_blocks;
+  const int t0 = b % a.tiles0, t1 = (b / a.tiles0) % a.tiles1, t2 = b / (a.tiles0 * a.tiles1);
+  const int i00 = t0 * 32 + NGHOSTS, i10 = t1 * BY + NGHOSTS, z0 = t2 * P + NGHOSTS;
+  const int N0 = a.N0, top = NGHOSTS + a.Nxx1, zend = NGHOSTS + a.Nxx2;
+  const int N01 = (int)a.N01;
+  const T* __restrict__ u = a.S;
+  // ---- stage the planes, one row per warp iteration
+  const bool inner = (t0 == 0) || (i10 < 2 * NGHOSTS) || (i10 + BY + NGHOSTS > top);
+  for (int row = ty; row < P * NR; row += BY) {
+    const int r = row % NR, p = row / NR;
+    const int i1 = i10 - NGHOSTS + r, i2 = z0 + p;
+    if (i2 >= zend || i1 >= top + NGHOSTS) continue;  // never read
+    if (!inner) {
+      const T* src = u + (i00 - NGHOSTS) + N0 * i1 + N01 * i2;
+      su[p][r][tx] = __ldg(src + tx);
+      if (tx < RWS - 32 && i00 - NGHOSTS + 32 + tx < N0) su[p][r][32 + tx] = __ldg(src + 32 + tx);
+    } else {
+      for (int x = tx; x < RWS; x += 32) {
+        int j0 = i00 - NGHOSTS + x, j1 = i1;
+        if (j0 >= N0) continue;
+        bool flip = false;
+        if (j1 < NGHOSTS) {
+          j1 = 2 * NGHOSTS - 1 - j1;
+          flip = true;
+        } else if (j1 >= top) {
+          j1 = 2 * top - 1 - j1;
+          flip = true;
+        }
+        if (j0 < NGHOSTS) {
+          j0 = 2 * NGHOSTS - 1 - j0;
+          flip = !flip;
+        }
+        const int j2 = flip ? wrap2(i2 + a.half2, a.Nxx2) : i2;
+        su[p][r][x] = __ldg(u + j0 + N0 * j1 + N01 * j2);
+      }
+    }
+  }
+  const int i0 = i00 + tx, i1 = i10 + ty;
+  const bool valid = i0 < NGHOSTS + a.Nxx0 && i1 < top;
+  const int k2 = i0 + N0 * i1;
+  T col[P + 10];
+  T pf[8][P];
+  if (valid) {
+    // uu along i2 for planes z0-5 .. z0+P+4 (wrapped by 2 pi)
+#pragma unroll
+    for (int q = 0; q < P + 10; q++) col[q] = __ldg(u + k2 + N01 * wrap2(z0 - 5 + q, a.Nxx2));
+    const long long Ntot = a.Ntot;
+#pragma unroll
+    for (int p = 0; p < P; p++) {
+      const int idx = k2 + N01 * (z0 + p < zend ? z0 + p : z0);
+      pf[0][p] = __ldg(a.S + Ntot + idx);
+      pf[1][p] = __ldg(a.aux + ADD_TIMES_AUUGF * Ntot + idx);
+      pf[2][p] = __ldg(a.aux + PSI_BACKGROUNDGF * Ntot + idx);
+      pf[3][p] = __ldg(a.aux + WAVESPEEDGF * Ntot + idx);
+      pf[4][p] = a.y[idx];
+      pf[5][p] = a.y[Ntot + idx];
+      pf[6][p] = (STAGE == 1) ? (T)0 : a.acc[idx];
+      pf[7][p] = (STAGE == 1) ? (T)0 : a.acc[Ntot + idx];
+    }
+  }
+  __syncthreads();
+  double r2 = 0.0;
+  if (valid) {
+    const T C22 = __ldg(a.coef + k2), C00 = __ldg(a.coef + N01 + k2), C11 = __ldg(a.coef + 2 * N01 + k2);
+    const T C1 = __ldg(a.coef + 3 * N01 + k2), C0 = __ldg(a.coef + 4 * N01 + k2), Cc = __ldg(a.coef + 5 * N01 + k2);
+#pragma unroll
+    for (int p = 0; p < P; p++) {
+      const int i2 = z0 + p;
+      if (i2 < zend) {
+        const T* sp = &su[p][ty + NGHOSTS][tx + NGHOSTS];
+        T s0 = 0, s1 = 0, s00 = 0, s11 = 0, s22 = 0;
+#pragma unroll
+        for (int k = 1; k <= 5; k++) {
+          const T am = sp[-k], ap = sp[k];
+          const T bm = sp[-k * RWS], bp = sp[k * RWS];
+          s0 = fma(W<T>::d(k), ap - am, s0);
+          s1 = fma(W<T>::d(k), bp - bm, s1);
+          s00 = fma(W<T>::e(k), ap + am, s00);
+          s11 = fma(W<T>::e(k), bp + bm, s11);
+        }
+#pragma unroll
+        for (int k = 1; k <= 5; k++) s22 = fma(W<T>::e(k), col[p + 5 + k] + col[p + 5 - k], s22);
+        T ku, kv, br;
+        point_rhs<T>(col[p + 5], pf[0][p], pf[1][p], pf[2][p], pf[3][p], C22, C00, C11, C1, C0, Cc, s0, s1, s00, s11,
+                     s22, a.eta, ku, kv, br);
+        store_point<T, STAGE>(a, k2 + (long long)N01 * i2, ku, kv, pf[4][p], pf[5][p], pf[6][p], pf[7][p]);
+        if (RESID) {
+          const double bb = (double)br;
+          r2 += bb * bb * __ldg(a.w + k2);
+        }
+      }
+    }
+  }
+  if (RESID && tile_partial<NT>(r2, b, a.partials, a.ticket, a.n_tiles, sh, &last)) finalize_l2<T, NT>(a, sh);
 }
 
 // Inner ghost points of gfs copied from their sources (apply_bcs_inner_only);
@@ -381,10 +365,18 @@ __global__ void k_ghost_fill(const int2* __restrict__ map, const signed char* __
 
 // ------------------------------------------------------------------ tiles
 
+// kind 0: direct; 2: direct with the pointwise inputs of all P planes loaded
+// up front; 3: TMA pipeline (kernels_bulk.cu) shape v, FP64 on grids with an
+// even row length and 16-byte aligned arrays, else kind 2 (4, 2); 4: planes
+// in shared memory (its column blocks by rows, column_rows).
 struct TileShape {
-  int by, p;
+  int by, p, kind, v;
 };
-static const TileShape kTiles[] = {{4, 1}, {4, 2}, {2, 4}, {8, 1}, {8, 2}, {4, 4}};
+static const TileShape kTiles[] = {{4, 1, 0, 0}, {4, 2, 0, 0}, {2, 4, 0, 0}, {8, 1, 0, 0}, {8, 2, 0, 0},
+                                   {4, 4, 0, 0}, {4, 1, 2, 0}, {4, 2, 2, 0}, {2, 4, 2, 0}, {4, 4, 2, 0},
+                                   {8, 2, 2, 0}, {4, 4, 3, 0}, {4, 4, 3, 1}, {8, 2, 3, 2}, {2, 8, 3, 3},
+                                   {4, 2, 3, 4}, {4, 2, 4, 0}, {4, 4, 4, 0}, {8, 2, 4, 0}, {2, 4, 4, 0},
+                                   {8, 1, 4, 0}, {4, 1, 4, 0}, {8, 4, 4, 0}};
 constexpr int kNumTiles = sizeof(kTiles) / sizeof(kTiles[0]);
 
 int substep_num_tiles() { return kNumTiles; }
@@ -393,76 +385,103 @@ void substep_tile_shape(int tile, int* bx, int* by, int* p) {
   *by = kTiles[tile].by;
   *p = kTiles[tile].p;
 }
+int substep_tile_kind(int tile) { return kTiles[tile].kind; }
 
 int substep_interior_blocks(const Dims& d, int tile) {
   const TileShape s = kTiles[tile];
   return ((d.Nxx0 + 31) / 32) * ((d.Nxx1 + s.by - 1) / s.by) * ((d.Nxx2 + s.p - 1) / s.p);
 }
 
-template <typename T>
-static SubDev<T> make_dev(const SubstepArgs& a) {
-  const TileShape ts = kTiles[a.tile];
-  SubDev<T> f;
-  const Dims& d = a.d;
-  f.N0 = d.N0;
-  f.N1 = d.N1;
-  f.Nxx0 = d.Nxx0;
-  f.Nxx1 = d.Nxx1;
-  f.Nxx2 = d.Nxx2;
-  f.half2 = d.Nxx2 / 2;
-  f.N01 = (long long)d.N0 * d.N1;
-  f.Ntot = d.Ntot;
-  f.tiles0 = (d.Nxx0 + 31) / 32;
-  f.tiles1 = (d.Nxx1 + ts.by - 1) / ts.by;
-  f.tiles2 = (d.Nxx2 + ts.p - 1) / ts.p;
-  f.n_int_blocks = f.tiles0 * f.tiles1 * f.tiles2;
-  f.ncol = d.Nxx1 * d.Nxx2;
-  f.S = (const T*)a.S;
-  f.y = (const T*)a.y;
-  f.acc = (T*)a.acc;
-  f.out = (T*)a.out;
-  f.aux = (const T*)a.aux;
-  f.coef = sizeof(T) == 8 ? (const T*)a.rt->coef : (const T*)a.rt->coef32;
-  f.colgeo = a.bt->colgeo;
-  f.w = a.lt ? a.lt->w : nullptr;
-  f.partials = a.s->partials;
-  f.ticket = a.s->counter;
-  f.state = a.state;
-  f.history = a.history;
-  f.done = a.done;
-  f.volume = a.lt ? a.lt->volume : 1.0;
-  f.log10_tol = a.log10_tol;
-  f.max_steps = a.max_steps;
-  f.stall = a.stall;
-  f.stall_window = a.stall_window;
-  f.stall_log_drop = a.stall_log_drop;
-  f.dt = (T)a.dt;
-  f.eta = (T)a.eta;
-  f.cOB[0] = (T)a.cOB[0];
-  f.cOB[1] = (T)a.cOB[1];
-  f.invdx0 = a.rt->invdx[0];
-  f.invdx1 = a.rt->invdx[1];
-  return f;
-}
-
-template <typename T, int STAGE, bool RESID, int BY, int P>
-static void launch_one(const SubstepArgs& a) {
-  SubDev<T> f = make_dev<T>(a);
+template <typename T, int STAGE, bool RESID, int BY, int P, bool PF>
+static void launch_direct(const SubstepArgs& a) {
+  SubDev<T> f = make_dev<T>(a, BY, P);
   constexpr int NT = 32 * BY;
   constexpr int CB = NT / kColThreadsPerColumn;
   f.n_col_blocks = (f.ncol + CB - 1) / CB;
-  NRPYELL_LAUNCH((k_substep<T, STAGE, RESID, BY, P>), f.n_int_blocks + f.n_col_blocks, NT, 0, f);
+  NRPYELL_LAUNCH((k_substep<T, STAGE, RESID, BY, P, PF>), f.n_tiles + f.n_col_blocks, NT, 0, f);
 }
+
+template <typename T, int STAGE, bool RESID, int BY, int P>
+static void launch_planes(const SubstepArgs& a) {
+  SubDev<T> f = make_dev<T>(a, BY, P);
+  constexpr int NT = 32 * BY;
+  f.n_col_blocks = ((a.d.Nxx1 + kRows - 1) / kRows) * a.d.Nxx2;
+  NRPYELL_LAUNCH((k_substep_planes<T, STAGE, RESID, BY, P>), f.n_tiles + f.n_col_blocks, NT, 0, f);
+}
+
+static cudaEvent_t g_fork = nullptr, g_join = nullptr;
+
+void prepare_columns() {
+  side_stream();
+  if (!g_fork) {
+    NRPYELL_CUDA(cudaEventCreateWithFlags(&g_fork, cudaEventDisableTiming));
+    NRPYELL_CUDA(cudaEventCreateWithFlags(&g_join, cudaEventDisableTiming));
+  }
+}
+
+template <typename T>
+void launch_columns_forked(int stage, const SubstepArgs& a) {
+  prepare_columns();
+  SubDev<T> f = make_dev<T>(a, 4, 1);
+  f.n_col_blocks = 0;
+  const int grid = ((a.d.Nxx1 + kRows - 1) / kRows) * a.d.Nxx2;
+  cudaStream_t side = side_stream();
+  NRPYELL_CUDA(cudaEventRecord(g_fork, stream()));
+  NRPYELL_CUDA(cudaStreamWaitEvent(side, g_fork, 0));
+  switch (stage) {
+    case 1: NRPYELL_LAUNCH_ON(side, (k_radiation_rows<T, 1>), grid, 128, 0, f); break;
+    case 2: NRPYELL_LAUNCH_ON(side, (k_radiation_rows<T, 2>), grid, 128, 0, f); break;
+    case 3: NRPYELL_LAUNCH_ON(side, (k_radiation_rows<T, 3>), grid, 128, 0, f); break;
+    default: NRPYELL_LAUNCH_ON(side, (k_radiation_rows<T, 4>), grid, 128, 0, f); break;
+  }
+}
+template void launch_columns_forked<double>(int, const SubstepArgs&);
+template void launch_columns_forked<float>(int, const SubstepArgs&);
+
+void join_columns() {
+  NRPYELL_CUDA(cudaEventRecord(g_join, side_stream()));
+  NRPYELL_CUDA(cudaStreamWaitEvent(stream(), g_join, 0));
+}
+
+template <typename T>
+void prepare_substep(int tile) {
+  if (kTiles[tile].kind == 3) prepare_bulk(kTiles[tile].v);
+}
+template void prepare_substep<double>(int);
+template void prepare_substep<float>(int);
 
 template <typename T, int STAGE, bool RESID>
 static void launch_tile(const SubstepArgs& a) {
   switch (a.tile) {
-    case 0: launch_one<T, STAGE, RESID, 4, 1>(a); break;
-    case 1: launch_one<T, STAGE, RESID, 4, 2>(a); break;
-    case 2: launch_one<T, STAGE, RESID, 2, 4>(a); break;
-    case 3: launch_one<T, STAGE, RESID, 8, 1>(a); break;
-    case 4: launch_one<T, STAGE, RESID, 8, 2>(a); break;
-    default: launch_one<T, STAGE, RESID, 4, 4>(a); break;
+    case 0: launch_direct<T, STAGE, RESID, 4, 1, false>(a); break;
+    case 1: launch_direct<T, STAGE, RESID, 4, 2, false>(a); break;
+    case 2: launch_direct<T, STAGE, RESID, 2, 4, false>(a); break;
+    case 3: launch_direct<T, STAGE, RESID, 8, 1, false>(a); break;
+    case 4: launch_direct<T, STAGE, RESID, 8, 2, false>(a); break;
+    case 5: launch_direct<T, STAGE, RESID, 4, 4, false>(a); break;
+    case 6: launch_direct<T, STAGE, RESID, 4, 1, true>(a); break;
+    case 7: launch_direct<T, STAGE, RESID, 4, 2, true>(a); break;
+    case 8: launch_direct<T, STAGE, RESID, 2, 4, true>(a); break;
+    case 9: launch_direct<T, STAGE, RESID, 4, 4, true>(a); break;
+    case 10: launch_direct<T, STAGE, RESID, 8, 2, true>(a); break;
+    case 11:
+    case 12:
+    case 13:
+    case 14:
+    case 15:
+      if (bulk_available(a, sizeof(T)))
+        launch_bulk(STAGE, kTiles[a.tile].v, a);
+      else
+        launch_direct<T, STAGE, RESID, 4, 2, true>(a);
+      break;
+    case 16: launch_planes<T, STAGE, RESID, 4, 2>(a); break;
+    case 17: launch_planes<T, STAGE, RESID, 4, 4>(a); break;
+    case 18: launch_planes<T, STAGE, RESID, 8, 2>(a); break;
+    case 19: launch_planes<T, STAGE, RESID, 2, 4>(a); break;
+    case 20: launch_planes<T, STAGE, RESID, 8, 1>(a); break;
+    case 21: launch_planes<T, STAGE, RESID, 4, 1>(a); break;
+    case 22: launch_planes<T, STAGE, RESID, 8, 4>(a); break;
+    default: NRPYELL_FAIL("launch_substep: tile index out of range"); break;
   }
 }
 

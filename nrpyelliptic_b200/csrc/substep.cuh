@@ -1,0 +1,421 @@
+// Device code shared by the fused RK4 substep kernels (kernels_fused.cu: one
+// thread per (i0,i1) column of P points reading through L1; kernels_bulk.cu:
+// tiles staged in shared memory by bulk asynchronous copies): the launch
+// arguments, the point RHS, the RK combination, the radiation-BC column work
+// and the stop-test reduction.  Every variant evaluates a point with the same
+// operations in the same order, so all of them produce identical bits.
+#pragma once
+
+#include "fd_weights.h"
+#include "kernels.cuh"
+
+namespace nrpyell {
+
+// Upwind first-derivative weights (one copy per translation unit).
+static __constant__ double c_fd1w[11][11] = NRPYELL_FD1_UPWIND_INIT;
+
+template <typename T>
+struct SubDev {
+  int N0, N1, Nxx0, Nxx1, Nxx2, half2;
+  long long N01, Ntot;
+  int tiles0, tiles1, tiles2;  // interior tile grid
+  int n_tiles, n_col_blocks, ncol;
+  const T* __restrict__ S;     // stage input
+  const T* y;                  // y_n (aliases out at stage 4)
+  T* acc;
+  T* out;
+  const T* __restrict__ aux;
+  const T* __restrict__ coef;
+  const double* __restrict__ colgeo;
+  const double* __restrict__ w;  // L2 weights (stage-1 residual)
+  double* partials;
+  unsigned int* ticket;
+  int* state;  // [0] n, [1] done, [2] converged, [3] stalled
+  int* err;    // set to a nonzero code when a bounded wait gives up
+  double* history;
+  const int* done;
+  double volume, log10_tol;
+  int max_steps;
+  double* stall;
+  int stall_window;
+  double stall_log_drop;
+  T dt, eta;
+  T cOB[2];
+  double invdx0, invdx1;
+};
+
+// Interior index along i2 after a wrap by 2 pi.
+__device__ __forceinline__ int wrap2(int j, int Nxx2) {
+  j -= NGHOSTS;
+  if (j < 0) j += Nxx2;
+  if (j >= Nxx2) j -= Nxx2;
+  return j + NGHOSTS;
+}
+
+template <typename T, int STAGE>
+__device__ __forceinline__ void rk_combine(T k, T yv, T& acc, T& out, T dt) {
+  const T dk = dt * k;
+  if (STAGE == 1) {
+    acc = (T)(1.0 / 6.0) * dk;
+    out = fma((T)0.5, dk, yv);
+  } else if (STAGE == 2) {
+    acc = fma((T)(1.0 / 3.0), dk, acc);
+    out = fma((T)0.5, dk, yv);
+  } else if (STAGE == 3) {
+    acc = fma((T)(1.0 / 3.0), dk, acc);
+    out = fma(dt, k, yv);
+  } else {
+    out = yv + fma((T)(1.0 / 6.0), dk, acc);
+  }
+}
+
+// 10th-order weights (rhs_eval.c:23-27): first derivative d_k, second e_k.
+template <typename T>
+struct W {
+  static __device__ __forceinline__ T d(int k) {
+    return k == 1 ? (T)(5.0 / 6.0) : k == 2 ? (T)(-5.0 / 21.0) : k == 3 ? (T)(5.0 / 84.0) : k == 4 ? (T)(-5.0 / 504.0) : (T)(1.0 / 1260.0);
+  }
+  static __device__ __forceinline__ T e(int k) {
+    return k == 1 ? (T)(5.0 / 3.0) : k == 2 ? (T)(-5.0 / 21.0) : k == 3 ? (T)(5.0 / 126.0) : k == 4 ? (T)(-5.0 / 1008.0) : (T)(1.0 / 3150.0);
+  }
+};
+
+// RHS of (uu, vv) at one interior point from the raw stencil sums and the
+// pointwise values.  Every variant and the column blocks call this with the
+// stencil sums accumulated in the same order, so all produce identical bits.
+template <typename T>
+__device__ __forceinline__ void point_rhs(T c, T vv, T AA, T psi, T ws, T C22, T C00, T C11, T C1, T C0, T Cc,
+                                          T s0, T s1, T s00, T s11, T s22, T eta, T& ku, T& kv, T& bracket) {
+  const T pu = psi + c;
+  const T pu2 = pu * pu;
+  const T pu4 = pu2 * pu2;
+  const T pu7 = pu4 * pu2 * pu;
+  T lap = Cc * c;
+  lap = fma(C00, s00, lap);
+  lap = fma(C11, s11, lap);
+  lap = fma(C22, s22, lap);
+  lap = fma(C1, s1, lap);
+  lap = fma(C0, s0, lap);
+  bracket = fma((T)0.125, AA / pu7, lap);
+  ku = fma(-eta, c, vv);
+  kv = (ws * ws) * bracket;
+}
+
+// Loads the pointwise values at idx / k2 and evaluates point_rhs.
+template <typename T>
+__device__ __forceinline__ void point_rhs_global(const SubDev<T>& a, long long idx, int k2, T c, T s0, T s1, T s00,
+                                                 T s11, T s22, T& ku, T& kv, T& bracket) {
+  const long long n01 = a.N01;
+  point_rhs<T>(c, __ldg(a.S + a.Ntot + idx), __ldg(a.aux + ADD_TIMES_AUUGF * a.Ntot + idx),
+               __ldg(a.aux + PSI_BACKGROUNDGF * a.Ntot + idx), __ldg(a.aux + WAVESPEEDGF * a.Ntot + idx),
+               __ldg(a.coef + k2), __ldg(a.coef + n01 + k2), __ldg(a.coef + 2 * n01 + k2), __ldg(a.coef + 3 * n01 + k2),
+               __ldg(a.coef + 4 * n01 + k2), __ldg(a.coef + 5 * n01 + k2), s0, s1, s00, s11, s22, a.eta, ku, kv,
+               bracket);
+}
+
+// Stencil sums along i0 and i1 at interior point (i0,i1,i2) from global
+// memory; ghost neighbours are read from their source points.  i2h is the i2
+// index shifted by pi.
+template <typename T>
+__device__ __forceinline__ void stencil01(const SubDev<T>& a, const T* __restrict__ u, int i0, int i1, int i2, int i2h,
+                                          T& s0, T& s1, T& s00, T& s11) {
+  const long long base = i0 + (long long)a.N0 * i1 + a.N01 * i2;
+  const long long rowh = (long long)a.N0 * i1 + a.N01 * i2h;  // (.,i1,i2h)
+  const long long colh = i0 + a.N01 * i2h;                     // (i0,.,i2h)
+  const int top = NGHOSTS + a.Nxx1;
+#pragma unroll
+  for (int k = 1; k <= 5; k++) {
+    const int j0 = i0 - k;
+    const long long im = (j0 >= NGHOSTS) ? base - k : (2 * NGHOSTS - 1 - j0) + rowh;
+    const int jm = i1 - k, jp = i1 + k;
+    const long long jmi = (jm >= NGHOSTS) ? base - (long long)k * a.N0 : colh + (long long)a.N0 * (2 * NGHOSTS - 1 - jm);
+    const long long jpi = (jp < top) ? base + (long long)k * a.N0 : colh + (long long)a.N0 * (2 * top - 1 - jp);
+    const T am = __ldg(u + im), ap = __ldg(u + base + k);
+    const T bm = __ldg(u + jmi), bp = __ldg(u + jpi);
+    s0 = fma(W<T>::d(k), ap - am, s0);
+    s1 = fma(W<T>::d(k), bp - bm, s1);
+    s00 = fma(W<T>::e(k), ap + am, s00);
+    s11 = fma(W<T>::e(k), bp + bm, s11);
+  }
+}
+
+// RK combination and stores of both gridfunctions at one interior point.
+template <typename T, int STAGE>
+__device__ __forceinline__ void store_point(const SubDev<T>& a, long long idx, T ku, T kv, T yu, T yv, T accu, T accv) {
+  T ou, ov;
+  rk_combine<T, STAGE>(ku, yu, accu, ou, a.dt);
+  rk_combine<T, STAGE>(kv, yv, accv, ov, a.dt);
+  if (STAGE != 4) {
+    a.acc[idx] = accu;
+    a.acc[a.Ntot + idx] = accv;
+  }
+  a.out[idx] = ou;
+  a.out[a.Ntot + idx] = ov;
+}
+
+// Barrier over the NT threads that reduce: the whole block, or (bulk kernel)
+// the consumer warps only, on a named barrier.
+struct BlockSync {
+  static __device__ __forceinline__ void sync() { __syncthreads(); }
+};
+template <int ID, int NT>
+struct NamedSync {
+  static __device__ __forceinline__ void sync() { asm volatile("bar.sync %0, %1;\n" ::"n"(ID), "n"(NT) : "memory"); }
+};
+
+// Stop test: the block that completes the last tile sums the per-tile
+// partials in index order, writes log10 L2 to history[n] and updates state.
+// Threads 0..NT-1 take part.
+template <typename T, int NT, class Sync = BlockSync>
+__device__ void finalize_l2(const SubDev<T>& a, double* sh) {
+  const int tid = threadIdx.x;
+  __threadfence();
+  double v = 0.0;
+  for (int i = tid; i < a.n_tiles; i += NT) v += ((volatile double*)a.partials)[i];
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
+  Sync::sync();
+  if ((tid & 31) == 0) sh[tid >> 5] = v;
+  Sync::sync();
+  if (tid == 0) {
+    double tot = 0.0;
+    for (int wi = 0; wi < NT / 32; wi++) tot += sh[wi];
+    const double l2 = log10(1e-16 + sqrt(tot / a.volume));
+    const int n = a.state[0];
+    if (a.history) a.history[n] = l2;
+    // Stall test on the best residual so far: the relaxation residual
+    // oscillates (and grows for a while after a cold start), so only a lack
+    // of progress of the running minimum over a whole window counts, and only
+    // once that minimum is within two decades of the tolerance of this phase
+    // -- a precision floor shows up there.
+    bool stalled = false;
+    if (a.stall_window > 0) {
+      if (n == 0 || l2 < a.stall[0] + a.stall_log_drop) {
+        a.stall[0] = l2;
+        a.stall[1] = (double)n;
+      } else if (n - (int)a.stall[1] >= a.stall_window && a.stall[0] <= a.log10_tol + 2.0) {
+        stalled = true;
+      }
+    }
+    if (l2 <= a.log10_tol) {
+      a.state[2] = 1;
+      a.state[1] = 1;
+    } else if (stalled) {
+      a.state[3] = 1;
+      a.state[1] = 1;
+    } else if (n >= a.max_steps) {
+      a.state[1] = 1;
+    } else {
+      a.state[0] = n + 1;
+    }
+    *a.ticket = 0u;
+    __threadfence();
+  }
+}
+
+// Reduces r2 over threads 0..NT-1, stores the tile's partial and returns
+// true in each of them if this tile was the last one to complete.
+template <int NT, class Sync = BlockSync>
+__device__ __forceinline__ bool tile_partial(double r2, int tile, double* partials, unsigned int* ticket, int n_tiles,
+                                             double* sh, bool* last) {
+  const int tid = threadIdx.x;
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) r2 += __shfl_down_sync(0xffffffffu, r2, o);
+  if ((tid & 31) == 0) sh[tid >> 5] = r2;
+  Sync::sync();
+  if (tid == 0) {
+    double t = 0.0;
+    for (int wi = 0; wi < NT / 32; wi++) t += sh[wi];
+    partials[tile] = t;
+    __threadfence();
+    *last = (atomicAdd(ticket, 1u) == (unsigned)n_tiles - 1);
+  }
+  Sync::sync();
+  return *last;
+}
+
+// ------------------------------------------------------------------ columns
+constexpr int kColThreadsPerColumn = 16;
+
+// Raw 11-point first-derivative sums of the radiation BC: along x0 with the
+// weights w of the point's stencil offset, along x1 with the centred weights
+// (the centre term is zero).  v holds the 11 values in stencil order.
+__device__ __forceinline__ double radiation_sum_x0(const double* w, const double* v) {
+  double d = w[0] * v[0];
+#pragma unroll
+  for (int m = 1; m < 11; m++) d = d + w[m] * v[m];
+  return d;
+}
+__device__ __forceinline__ double radiation_sum_x1(const double* v) {
+  double d = c_fd1w[5][0] * v[0];
+#pragma unroll
+  for (int m = 1; m < 11; m++)
+    if (m != 5) d = d + c_fd1w[5][m] * v[m];
+  return d;
+}
+
+// d f/d r at one radiation point from the raw x0 / x1 stencil sums.
+__device__ __forceinline__ double radiation_drf(double d0, double d1, double invdx0, double invdx1, double dx0dr,
+                                                double dx1dr) {
+  d0 *= invdx0;
+  d1 *= invdx1;
+  return dx0dr * d0 + dx1dr * d1;
+}
+
+// RHS of one gridfunction on the five outer layers of a column, inner to
+// outer (apply_bcs_outerradiation_and_inner.c:400-407): kprev is the RHS of
+// the last interior point, drf/fvs the radial derivative and value at the
+// last interior point (index 0) and at layers 0..4 (1..5); colgeo the
+// column's radial geometry (r at index 0..5, stride N1).
+__device__ __forceinline__ void radiation_layers(double cw, double kprev, const double* drf, const double* fvs,
+                                                 const double* __restrict__ rcol, int N1, double* kk) {
+#pragma unroll
+  for (int L = 0; L < NGHOSTS; L++) {
+    const double rn = __ldg(rcol + L * N1);
+    const double rr = __ldg(rcol + (L + 1) * N1);
+    const double out_int = -cw * (drf[L] + fvs[L] / rn);
+    const double K = rn * rn * rn * (kprev - out_int);
+    const double rinv = 1.0 / rr;
+    const double outw = -cw * (drf[L + 1] + fvs[L + 1] * rinv);
+    const double k = outw + K * rinv * rinv * rinv;
+    kk[L] = k;
+    kprev = k;
+  }
+}
+
+// Radiation BC for CB columns (block-local index cb).  Column c, task r:
+// r < 12 -> d f/d r at point jj = r % 6 of gridfunction g = r / 6 (point jj
+// is i0 = N0-6+jj; jj = 0 is the last interior plane, jj = 1..5 the outer
+// layers 0..4); r == 12 -> RHS at the last interior point.  The upwind x0
+// stencil at point jj has offset -1 for jj <= 1 and -jj otherwise
+// (compute_partial_r_f's rule); the x1 stencil is centred.  The "interior
+// neighbour" derivative of layer L is the point derivative of layer L-1.
+template <typename T, int STAGE, int NT>
+__device__ void column_block(const SubDev<T>& a, int cb) {
+  constexpr int CB = NT / kColThreadsPerColumn;
+  __shared__ double drf[CB][2][6], fvs[CB][2][6], kl[CB][2], kk[CB][2][5];
+  const int tid = threadIdx.x;
+  const int c = tid / kColThreadsPerColumn, r = tid % kColThreadsPerColumn;
+  const int colid = cb * CB + c;
+  const bool live = colid < a.ncol;
+  const int i1 = NGHOSTS + (live ? colid % a.Nxx1 : 0);
+  const int i2 = NGHOSTS + (live ? colid / a.Nxx1 : 0);
+  const int i2h = wrap2(i2 + a.half2, a.Nxx2);
+  const int N0 = a.N0;
+  const long long row = (long long)N0 * i1 + a.N01 * i2;
+  if (live && r < 12) {
+    const int g = r / 6, jj = r % 6;
+    const T* f = a.S + g * a.Ntot;
+    const int ip = N0 - 6 + jj;
+    const int off = (jj <= 1) ? -1 : -jj;
+    double v[11];
+#pragma unroll
+    for (int m = 0; m < 11; m++) v[m] = (double)__ldg(f + row + ip + off - 5 + m);
+    const double d0 = radiation_sum_x0(c_fd1w[off + 5], v);
+    // centred x1 stencil; points across the axis come from their images
+    const int top = NGHOSTS + a.Nxx1;
+#pragma unroll
+    for (int m = 0; m < 11; m++) {
+      const int j1 = i1 + m - 5;
+      long long id;
+      if (j1 < NGHOSTS)
+        id = ip + (long long)N0 * (2 * NGHOSTS - 1 - j1) + a.N01 * i2h;
+      else if (j1 >= top)
+        id = ip + (long long)N0 * (2 * top - 1 - j1) + a.N01 * i2h;
+      else
+        id = ip + (long long)N0 * j1 + a.N01 * i2;
+      v[m] = (m == 5) ? 0.0 : (double)__ldg(f + id);
+    }
+    const double d1 = radiation_sum_x1(v);
+    drf[c][g][jj] = radiation_drf(d0, d1, a.invdx0, a.invdx1, __ldg(a.colgeo + (1 * 6 + jj) * a.N1 + i1),
+                                  __ldg(a.colgeo + (2 * 6 + jj) * a.N1 + i1));
+    fvs[c][g][jj] = (double)__ldg(f + row + ip);
+  } else if (live && r == 12) {
+    const int i0 = N0 - NGHOSTS - 1;
+    const T* u = a.S;
+    const long long idx = row + i0;
+    T s0 = 0, s1 = 0, s00 = 0, s11 = 0, s22 = 0;
+    stencil01<T>(a, u, i0, i1, i2, i2h, s0, s1, s00, s11);
+    const long long line = i0 + (long long)N0 * i1;
+#pragma unroll
+    for (int k = 1; k <= 5; k++)
+      s22 = fma(W<T>::e(k),
+                __ldg(u + line + a.N01 * wrap2(i2 + k, a.Nxx2)) + __ldg(u + line + a.N01 * wrap2(i2 - k, a.Nxx2)), s22);
+    T ku, kv, br;
+    point_rhs_global<T>(a, idx, i0 + N0 * i1, __ldg(u + idx), s0, s1, s00, s11, s22, ku, kv, br);
+    kl[c][0] = (double)ku;
+    kl[c][1] = (double)kv;
+  }
+  __syncthreads();
+  if (live && r < 2) {
+    const int g = r;
+    radiation_layers((double)a.cOB[g], kl[c][g], drf[c][g], fvs[c][g], a.colgeo + i1, a.N1, kk[c][g]);
+  }
+  __syncthreads();
+  if (live && r < 10) {
+    const int g = r / 5, L = r % 5;
+    const long long idx = g * a.Ntot + row + N0 - NGHOSTS + L;
+    T accv = (STAGE == 1) ? (T)0 : a.acc[idx];
+    T ov;
+    rk_combine<T, STAGE>((T)kk[c][g][L], a.y[idx], accv, ov, a.dt);
+    if (STAGE != 4) a.acc[idx] = accv;
+    a.out[idx] = ov;
+  }
+}
+
+// Interior index along i2 for any j (a tile that runs past the last plane
+// can reach more than one wrap on short grids).
+__device__ __forceinline__ int wrapm(int j, int Nxx2) {
+  j -= NGHOSTS;
+  while (j < 0) j += Nxx2;
+  while (j >= Nxx2) j -= Nxx2;
+  return j + NGHOSTS;
+}
+
+template <typename T>
+inline SubDev<T> make_dev(const SubstepArgs& a, int by, int p) {
+  SubDev<T> f;
+  const Dims& d = a.d;
+  f.N0 = d.N0;
+  f.N1 = d.N1;
+  f.Nxx0 = d.Nxx0;
+  f.Nxx1 = d.Nxx1;
+  f.Nxx2 = d.Nxx2;
+  f.half2 = d.Nxx2 / 2;
+  f.N01 = (long long)d.N0 * d.N1;
+  f.Ntot = d.Ntot;
+  f.tiles0 = (d.Nxx0 + 31) / 32;
+  f.tiles1 = (d.Nxx1 + by - 1) / by;
+  f.tiles2 = (d.Nxx2 + p - 1) / p;
+  f.n_tiles = f.tiles0 * f.tiles1 * f.tiles2;
+  f.ncol = d.Nxx1 * d.Nxx2;
+  f.S = (const T*)a.S;
+  f.y = (const T*)a.y;
+  f.acc = (T*)a.acc;
+  f.out = (T*)a.out;
+  f.aux = (const T*)a.aux;
+  f.coef = sizeof(T) == 8 ? (const T*)a.rt->coef : (const T*)a.rt->coef32;
+  f.colgeo = a.bt->colgeo;
+  f.w = a.lt ? a.lt->w : nullptr;
+  f.partials = a.s->partials;
+  f.ticket = a.s->counter;
+  f.state = a.state;
+  f.err = a.err;
+  f.history = a.history;
+  f.done = a.done;
+  f.volume = a.lt ? a.lt->volume : 1.0;
+  f.log10_tol = a.log10_tol;
+  f.max_steps = a.max_steps;
+  f.stall = a.stall;
+  f.stall_window = a.stall_window;
+  f.stall_log_drop = a.stall_log_drop;
+  f.dt = (T)a.dt;
+  f.eta = (T)a.eta;
+  f.cOB[0] = (T)a.cOB[0];
+  f.cOB[1] = (T)a.cOB[1];
+  f.invdx0 = a.rt->invdx[0];
+  f.invdx1 = a.rt->invdx[1];
+  return f;
+}
+
+}  // namespace nrpyell

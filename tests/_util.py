@@ -10,7 +10,7 @@ ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
 if ROOT not in sys.path:
     sys.path.insert(0, ROOT)
 
-from nrpyelliptic_b200 import abi  # noqa: E402
+from nrpyelliptic_b200 import _lib, abi  # noqa: E402
 
 GOLDEN = os.path.join(ROOT, "tests", "golden")
 P = C.POINTER
@@ -170,3 +170,52 @@ def relmax(a, b):
     """max |a-b| / max |b|"""
     a, b = np.asarray(a), np.asarray(b)
     return float(np.max(np.abs(a - b)) / max(np.max(np.abs(b)), 1e-300))
+
+
+class Dev:
+    """A device buffer holding a numpy array."""
+
+    def __init__(self, lib, a):
+        self.lib = lib
+        self.n = a.size
+        self.p = lib.nrpyell_device_malloc(a.nbytes)
+        _lib.check(lib)
+        self.set(a)
+
+    def set(self, a):
+        a = np.ascontiguousarray(a, dtype=np.float64)
+        self.lib.nrpyell_memcpy(self.p, a.ctypes.data, a.nbytes, 0)
+        _lib.check(self.lib)
+
+    def get(self):
+        out = np.empty(self.n)
+        self.lib.nrpyell_memcpy(out.ctypes.data, self.p, out.nbytes, 1)
+        _lib.check(self.lib)
+        return out
+
+    @property
+    def ptr(self):
+        return C.cast(C.c_void_p(self.p), abi.PREAL)
+
+    def __del__(self):
+        try:
+            self.lib.nrpyell_device_free(self.p)
+        except Exception:
+            pass
+
+
+def device_grid(lib, hg, y0):
+    """griddata_struct over device buffers: y_n = y0, aux from hg, zeroed RK buffers."""
+    bufs = {"y_n": Dev(lib, y0), "acc": Dev(lib, np.zeros(2 * hg.Ntot)), "k_odd": Dev(lib, np.zeros(2 * hg.Ntot)),
+            "k_even": Dev(lib, np.zeros(2 * hg.Ntot)), "aux": Dev(lib, hg.aux)}
+    g = abi.griddata_struct()
+    g.params = hg.params
+    for i in range(3):
+        g.xx[i] = hg.xx[i]
+    g.bcstruct = hg.bc
+    g.rfmstruct = hg.rfm
+    f = g.gridfuncs
+    f.y_n_gfs, f.y_nplus1_running_total_gfs = bufs["y_n"].ptr, bufs["acc"].ptr
+    f.k_odd_gfs, f.k_even_gfs, f.auxevol_gfs = bufs["k_odd"].ptr, bufs["k_even"].ptr, bufs["aux"].ptr
+    f.diagnostic_output_gfs = f.y_nplus1_running_total_gfs
+    return g, bufs

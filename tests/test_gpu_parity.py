@@ -14,45 +14,13 @@ import subprocess
 
 import numpy as np
 import pytest
-from _util import ROOT, golden_grid, interior_mask, load_golden, oracle, problem_grid, ptr, relmax
+from _util import ROOT, Dev, device_grid, golden_grid, interior_mask, load_golden, oracle, problem_grid, ptr, relmax
 
 from nrpyelliptic_b200 import _lib, abi
 from nrpyelliptic_b200.problem import CONFIGS, DeviceState, Problem
 
 pytestmark = pytest.mark.gpu
 CASES = ["ops_shipped_16x8x6.npz", "ops_unequal_24x16x8.npz"]
-
-
-class Dev:
-    """A device buffer holding a numpy array."""
-
-    def __init__(self, lib, a):
-        self.lib = lib
-        self.n = a.size
-        self.p = lib.nrpyell_device_malloc(a.nbytes)
-        _lib.check(lib)
-        self.set(a)
-
-    def set(self, a):
-        a = np.ascontiguousarray(a, dtype=np.float64)
-        self.lib.nrpyell_memcpy(self.p, a.ctypes.data, a.nbytes, 0)
-        _lib.check(self.lib)
-
-    def get(self):
-        out = np.empty(self.n)
-        self.lib.nrpyell_memcpy(out.ctypes.data, self.p, out.nbytes, 1)
-        _lib.check(self.lib)
-        return out
-
-    @property
-    def ptr(self):
-        return C.cast(C.c_void_p(self.p), abi.PREAL)
-
-    def __del__(self):
-        try:
-            self.lib.nrpyell_device_free(self.p)
-        except Exception:
-            pass
 
 
 @pytest.fixture(scope="module")
@@ -133,28 +101,12 @@ def test_inner_only_and_extrapolation_vs_oracle(lib, case):
     assert relmax(d.get(), yo) < 1e-15
 
 
-def _device_grid(lib, hg, y0):
-    bufs = {"y_n": Dev(lib, y0), "acc": Dev(lib, np.zeros(2 * hg.Ntot)), "k_odd": Dev(lib, np.zeros(2 * hg.Ntot)),
-            "k_even": Dev(lib, np.zeros(2 * hg.Ntot)), "aux": Dev(lib, hg.aux)}
-    g = abi.griddata_struct()
-    g.params = hg.params
-    for i in range(3):
-        g.xx[i] = hg.xx[i]
-    g.bcstruct = hg.bc
-    g.rfmstruct = hg.rfm
-    f = g.gridfuncs
-    f.y_n_gfs, f.y_nplus1_running_total_gfs = bufs["y_n"].ptr, bufs["acc"].ptr
-    f.k_odd_gfs, f.k_even_gfs, f.auxevol_gfs = bufs["k_odd"].ptr, bufs["k_even"].ptr, bufs["aux"].ptr
-    f.diagnostic_output_gfs = f.y_nplus1_running_total_gfs
-    return g, bufs
-
-
 @pytest.mark.parametrize("mode,tol1,tol10", [(1, 1e-13, 1e-12), (0, 1e-12, 1e-12)])
 @pytest.mark.parametrize("case", CASES)
 def test_mol_steps_vs_reference(lib, case, mode, tol1, tol10):
     gold = load_golden(case)
     hg = golden_grid(gold)
-    g, bufs = _device_grid(lib, hg, gold["y_consistent"])
+    g, bufs = device_grid(lib, hg, gold["y_consistent"])
     dt = float(gold["dt"])
     lib.nrpyell_set_step_mode(mode)
     try:
@@ -181,7 +133,7 @@ def test_mol_steps_production_grid_vs_oracle(lib, mode):
     o.oracle_apply_bcs_inner_only(C.byref(hg.params), C.byref(hg.bc), ptr(y))
     hg.bufs["y_n"][:] = y
     g_cpu = hg.griddata()
-    g, bufs = _device_grid(lib, hg, y)
+    g, bufs = device_grid(lib, hg, y)
     lib.nrpyell_set_step_mode(mode)
     try:
         for _ in range(20):
