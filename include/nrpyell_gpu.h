@@ -196,6 +196,16 @@ int nrpyell_relax_mixed(griddata_struct *griddata, const REAL dt, const REAL log
                         const REAL integration_radius, int *steps_fp32, int *steps_fp64, REAL *final_log10_l2,
                         REAL *history);
 
+/* Batched relaxation: n configurations, each a griddata_struct set up as for
+ * nrpyell_relax (its own grid size, parameters, bc_struct, rfm_struct and
+ * device gridfunctions; dt[c] its time step), relaxed together from their
+ * y_n_gfs to log10 L2 <= log10_tol or max_steps.  Every RK4 substep of all
+ * configurations is one kernel launch; each configuration stops on its own.
+ * steps_taken[c] and final_log10_l2[c] as in nrpyell_relax.  Returns the
+ * number of configurations that did not converge (0: all did), < 0 on
+ * error. */
+int nrpyell_relax_batch(int n, griddata_struct *grids, const REAL *dt, REAL log10_tol, int max_steps,
+                        REAL integration_radius, int *steps_taken, REAL *final_log10_l2);
 /* The same solve with host buffers: copies auxevol_host (3 gfs) and
  * y_n_host (2 gfs, the initial guess) to the device, relaxes, copies the
  * solution back into y_n_host. */

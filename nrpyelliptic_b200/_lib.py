@@ -77,6 +77,8 @@ EXPORTS = {
     "nrpyell_relax_mixed": (C.c_int, [P(abi.griddata_struct), C.c_double, C.c_double, C.c_double, C.c_int,
                                       C.c_double, C.c_int, C.c_double, P(C.c_int), P(C.c_int), P(C.c_double),
                                       PREAL]),
+    "nrpyell_relax_batch": (C.c_int, [C.c_int, P(abi.griddata_struct), PREAL, C.c_double, C.c_int, C.c_double,
+                                      P(C.c_int), PREAL]),
     "nrpyell_relax_host": (C.c_int, [P(abi.paramstruct), XX, P(abi.bc_struct), P(abi.rfm_struct), PREAL, PREAL,
                                      C.c_double, C.c_double, C.c_int, C.c_double, P(C.c_int), P(C.c_double)]),
 }

@@ -357,6 +357,7 @@ void nrpyell_release_tables(void) {
   if (g_stream) cudaStreamSynchronize(g_stream);
   release_graphs();
   release_work();
+  release_batch();
   release_all_tables();
 }
 

@@ -52,6 +52,7 @@ FusedWork* get_work(const Dims& d, int history_len);
 // Autotuned tile of a grid size (fp32: 0 or 1), -1 if not tuned yet.
 int find_tile(const Dims& d, int fp32);
 void release_work();
+void release_batch();  // batch.cu
 void release_graphs();
 bool fused_ready(const paramstruct* p, const rfm_struct* rfm, const bc_struct* bc, REAL* NRPYELL_RESTRICT const xx[3],
                  RfmTables** rt, BcTables** bt);

@@ -237,24 +237,28 @@ __global__ void __launch_bounds__(128) k_radiation_rows(SubDev<T> a) {
 // reads at compile-time offsets and the per-point integer work is small.
 // uu along i2 stays in registers and the pointwise inputs of all P planes are
 // loaded before the first store.
+// Shared memory of the planes kernel, in doubles: the planes of an interior
+// block, or the rows of a column block.
+template <typename T, int BY, int P>
+struct PlanesSmem {
+  static constexpr int planes = (P * (BY + 10) * 42 * (int)sizeof(T) + 7) / 8;
+  static constexpr int value = planes > kRowsSmem ? planes : kRowsSmem;
+};
+
+// Block `bid` of one grid's planes launch (column blocks first).
 template <typename T, int STAGE, bool RESID, int BY, int P>
-__global__ void __launch_bounds__(32 * BY) k_substep_planes(SubDev<T> a) {
+__device__ __forceinline__ void planes_block(const SubDev<T>& a, int bid, double* smem, double* sh, bool* lastp) {
   constexpr int NT = 32 * BY;
   constexpr int RWS = 42;       // i0 = i00-5 .. i00+36
   constexpr int NR = BY + 10;   // i1 = i10-5 .. i10+BY+4
-  constexpr int PLANES = (P * NR * RWS * (int)sizeof(T) + 7) / 8;
-  // the planes of an interior block, or the rows of a column block
-  __shared__ double smem[PLANES > kRowsSmem ? PLANES : kRowsSmem];
   T(*su)[NR][RWS] = reinterpret_cast<T(*)[NR][RWS]>(smem);
-  __shared__ double sh[NT / 32 > 8 ? NT / 32 : 8];
-  __shared__ bool last;
-  if (*a.done) return;
-  if ((int)blockIdx.x < a.n_col_blocks) {
-    column_rows<T, STAGE, NT>(a, blockIdx.x, smem);
+  bool& last = *lastp;
+  if (bid < a.n_col_blocks) {
+    column_rows<T, STAGE, NT>(a, bid, smem);
     return;
   }
   const int tid = threadIdx.x, tx = tid & 31, ty = tid >> 5;
-  const int b = blockIdx.x - a.n_col_blocks;
+  const int b = bid - a.n_col_blocks;
   const int t0 = b % a.tiles0, t1 = (b / a.tiles0) % a.tiles1, t2 = b / (a.tiles0 * a.tiles1);
   const int i00 = t0 * 32 + NGHOSTS, i10 = t1 * BY + NGHOSTS, z0 = t2 * P + NGHOSTS;
   const int N0 = a.N0, top = NGHOSTS + a.Nxx1, zend = NGHOSTS + a.Nxx2;
@@ -348,6 +352,38 @@ __global__ void __launch_bounds__(32 * BY) k_substep_planes(SubDev<T> a) {
     }
   }
   if (RESID && tile_partial<NT>(r2, b, a.partials, a.ticket, a.n_tiles, sh, &last)) finalize_l2<T, NT>(a, sh);
+}
+
+template <typename T, int STAGE, bool RESID, int BY, int P>
+__global__ void __launch_bounds__(32 * BY) k_substep_planes(SubDev<T> a) {
+  __shared__ double smem[PlanesSmem<T, BY, P>::value];
+  __shared__ double sh[BY > 8 ? BY : 8];
+  __shared__ bool last;
+  if (*a.done) return;
+  planes_block<T, STAGE, RESID, BY, P>(a, blockIdx.x, smem, sh, &last);
+}
+
+// One substep of many grids in one launch: the blocks of grid c are
+// offs[c] .. offs[c+1]-1 (column blocks first, then interior tiles), each
+// grid with its own launch arguments, stop test and done flag.
+template <typename T, int STAGE, bool RESID, int BY, int P>
+__global__ void __launch_bounds__(32 * BY)
+    k_substep_planes_batch(const SubDev<T>* __restrict__ devs, const int* __restrict__ offs, int n) {
+  __shared__ double smem[PlanesSmem<T, BY, P>::value];
+  __shared__ double sh[BY > 8 ? BY : 8];
+  __shared__ bool last;
+  int lo = 0, hi = n - 1;
+  const int bx = blockIdx.x;
+  while (lo < hi) {
+    const int mid = (lo + hi + 1) >> 1;
+    if (__ldg(offs + mid) <= bx)
+      lo = mid;
+    else
+      hi = mid - 1;
+  }
+  const SubDev<T>& a = devs[lo];
+  if (*a.done) return;
+  planes_block<T, STAGE, RESID, BY, P>(a, bx - __ldg(offs + lo), smem, sh, &last);
 }
 
 // Inner ghost points of gfs copied from their sources (apply_bcs_inner_only);
@@ -502,6 +538,57 @@ void launch_substep(int stage, const SubstepArgs& a) {
 }
 template void launch_substep<double>(int, const SubstepArgs&);
 template void launch_substep<float>(int, const SubstepArgs&);
+
+// ---------------------------------------------------------------- batches
+
+template <typename T>
+bool planes_launch_dev(const SubstepArgs& a, SubDev<T>* out) {
+  const int t = a.tile;
+  if (t < 0 || t >= kNumTiles || kTiles[t].kind != 4) {
+    NRPYELL_FAIL("batched substep: the tile must be a shared-memory planes shape");
+    return false;
+  }
+  *out = make_dev<T>(a, kTiles[t].by, kTiles[t].p);
+  out->n_col_blocks = ((a.d.Nxx1 + kRows - 1) / kRows) * a.d.Nxx2;
+  return true;
+}
+template bool planes_launch_dev<double>(const SubstepArgs&, SubDev<double>*);
+
+template <typename T, int STAGE, bool RESID>
+static void launch_batch_stage(int tile, const SubDev<T>* devs, const int* offs, int n, int blocks) {
+  const int by = kTiles[tile].by, p = kTiles[tile].p;
+#define NRPYELL_BATCH(BY, P)                                                                           \
+  if (by == BY && p == P) {                                                                            \
+    NRPYELL_LAUNCH((k_substep_planes_batch<T, STAGE, RESID, BY, P>), blocks, 32 * BY, 0, devs, offs, n); \
+    return;                                                                                            \
+  }
+  NRPYELL_BATCH(4, 2)
+  NRPYELL_BATCH(4, 4)
+  NRPYELL_BATCH(8, 2)
+  NRPYELL_BATCH(2, 4)
+  NRPYELL_BATCH(8, 1)
+  NRPYELL_BATCH(4, 1)
+  NRPYELL_BATCH(8, 4)
+#undef NRPYELL_BATCH
+  NRPYELL_FAIL("batched substep: no kernel for this tile shape");
+}
+
+template <typename T>
+void launch_substep_batch(int stage, bool resid, int tile, const SubDev<T>* devs, const int* offs, int n,
+                          int blocks) {
+  switch (stage) {
+    case 1:
+      if (resid)
+        launch_batch_stage<T, 1, true>(tile, devs, offs, n, blocks);
+      else
+        launch_batch_stage<T, 1, false>(tile, devs, offs, n, blocks);
+      break;
+    case 2: launch_batch_stage<T, 2, false>(tile, devs, offs, n, blocks); break;
+    case 3: launch_batch_stage<T, 3, false>(tile, devs, offs, n, blocks); break;
+    default: launch_batch_stage<T, 4, false>(tile, devs, offs, n, blocks); break;
+  }
+}
+template void launch_substep_batch<double>(int, bool, int, const SubDev<double>*, const int*, int, int);
 
 template <typename T>
 void launch_ghost_fill(const Dims& d, const BcTables* bt, void* gfs) {

@@ -1,0 +1,66 @@
+"""Batched relaxation (nrpyell_relax_batch): several configurations on
+grids of different sizes in one launch per substep give, configuration by
+configuration, the same solution and step count as relaxing each alone with
+the same tile shape."""
+import ctypes as C
+
+import numpy as np
+import pytest
+from _util import ptr
+
+from nrpyelliptic_b200 import _lib
+from nrpyelliptic_b200.batch import relax_batch
+from nrpyelliptic_b200.problem import CONFIGS, DeviceState, Problem, sample_sweep, with_grid
+
+pytestmark = pytest.mark.gpu
+PLANES_8x1 = 20  # a shared-memory planes tile shape (kind 4)
+
+
+@pytest.fixture(scope="module")
+def lib():
+    lib = _lib.load()
+    lib.nrpyell_clear_status()
+    yield lib
+    lib.nrpyell_set_tile(-1)
+
+
+def _alone(lib, prob, max_steps):
+    ds = DeviceState(prob, lib=lib)
+    steps, fin = C.c_int(0), C.c_double(0)
+    hist = np.zeros(max_steps + 1)
+    rc = lib.nrpyell_relax(C.byref(ds.g), prob.dt, -10.0, max_steps, prob.cfg.R_L2, C.byref(steps), C.byref(fin),
+                           ptr(hist))
+    _lib.check(lib)
+    y = ds.download("y_n")
+    ds.free()
+    return rc, steps.value, fin.value, y
+
+
+def test_batch_matches_single_runs(lib):
+    cfgs = [CONFIGS["shipped_64x64x8"], with_grid(CONFIGS["quasicircular_128x128x16"], (48, 48, 8)),
+            with_grid(sample_sweep(4)[1], (40, 24, 6)), CONFIGS["equal_mass_rest_64x64x8"]]
+    probs = [Problem(c, lib=lib) for c in cfgs]
+    lib.nrpyell_set_tile(PLANES_8x1)
+    try:
+        rc, steps, finals, states = relax_batch(probs, tol=-10.0, max_steps=8000, lib=lib)
+        assert rc == 0
+        assert steps[3] == 0  # the head-on pair at rest is solved by the zero guess
+        for i, p in enumerate(probs):
+            rc1, s1, f1, y1 = _alone(lib, p, 8000)
+            assert rc1 == 0
+            assert steps[i] == s1, (cfgs[i].name, steps[i], s1)
+            assert finals[i] == f1
+            np.testing.assert_array_equal(states[i].download("y_n"), y1, err_msg=cfgs[i].name)
+    finally:
+        lib.nrpyell_set_tile(-1)
+    for s in states:
+        s.free()
+
+
+def test_batch_autotuned_tile_converges(lib):
+    cfgs = [with_grid(c, (32, 32, 8)) for c in sample_sweep(6)]
+    probs = [Problem(c, lib=lib) for c in cfgs]
+    rc, steps, finals, states = relax_batch(probs, tol=-10.0, max_steps=20000, lib=lib)
+    assert rc == 0 and np.all(finals <= -10.0) and np.all(steps > 0)
+    for s in states:
+        s.free()
