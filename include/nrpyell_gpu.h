@@ -206,6 +206,29 @@ int nrpyell_relax_mixed(griddata_struct *griddata, const REAL dt, const REAL log
  * error. */
 int nrpyell_relax_batch(int n, griddata_struct *grids, const REAL *dt, REAL log10_tol, int max_steps,
                         REAL integration_radius, int *steps_taken, REAL *final_log10_l2);
+/* Learned initial guess (BF16 tensor-core MLP, FP32 master weights, Adam).
+ * The network maps n_in inputs through `depth` tanh layers of `width` to
+ * n_out linear outputs.  All arrays are device pointers unless named host.
+ * Parameters are stored layer by layer: W [in x out] row-major, then b. */
+void *nrpyell_mlp_create(int n_in, int width, int depth, int n_out, int batch_max, unsigned seed);
+void nrpyell_mlp_destroy(void *mlp);
+long long nrpyell_mlp_num_params(void *mlp);
+int nrpyell_mlp_get_params(void *mlp, float *host);
+int nrpyell_mlp_set_params(void *mlp, const float *host);
+/* y [n x n_out] = network(x [n x n_in]). */
+int nrpyell_mlp_predict(void *mlp, const float *x, int n, float *y);
+/* Mean squared error of one batch and its parameter gradient (copied to
+ * grad_host when non-NULL); 0 < rows <= batch_max. */
+double nrpyell_mlp_loss_grad(void *mlp, const float *x, const float *t, int rows, float *grad_host);
+/* Adam over `epochs` passes of seeded, shuffled minibatches (cosine decay of
+ * the learning rate to lr/100); returns the last epoch's mean loss and
+ * writes every epoch's to loss_history (host, optional). */
+double nrpyell_mlp_train(void *mlp, const float *x, const float *t, int n, int batch, int epochs, float lr,
+                         unsigned seed, double *loss_history);
+/* y_n of one configuration from K <= 4096 POD coefficients c: uu = mean +
+ * sum_k c_k basis_k (mean [Ntot], basis [K x Ntot], FP32), vv = eta uu. */
+int nrpyell_pod_guess(const float *mean, const float *basis, int K, long long ntot, const float *c, double eta,
+                      double *y_n);
 /* The same solve with host buffers: copies auxevol_host (3 gfs) and
  * y_n_host (2 gfs, the initial guess) to the device, relaxes, copies the
  * solution back into y_n_host. */

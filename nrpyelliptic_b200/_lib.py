@@ -79,6 +79,17 @@ EXPORTS = {
                                       PREAL]),
     "nrpyell_relax_batch": (C.c_int, [C.c_int, P(abi.griddata_struct), PREAL, C.c_double, C.c_int, C.c_double,
                                       P(C.c_int), PREAL]),
+    "nrpyell_mlp_create": (C.c_void_p, [C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, C.c_uint]),
+    "nrpyell_mlp_destroy": (None, [C.c_void_p]),
+    "nrpyell_mlp_num_params": (C.c_longlong, [C.c_void_p]),
+    "nrpyell_mlp_get_params": (C.c_int, [C.c_void_p, C.c_void_p]),
+    "nrpyell_mlp_set_params": (C.c_int, [C.c_void_p, C.c_void_p]),
+    "nrpyell_mlp_predict": (C.c_int, [C.c_void_p, C.c_void_p, C.c_int, C.c_void_p]),
+    "nrpyell_mlp_loss_grad": (C.c_double, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_int, C.c_void_p]),
+    "nrpyell_mlp_train": (C.c_double, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_int, C.c_int, C.c_int, C.c_float,
+                                       C.c_uint, C.c_void_p]),
+    "nrpyell_pod_guess": (C.c_int, [C.c_void_p, C.c_void_p, C.c_int, C.c_longlong, C.c_void_p, C.c_double,
+                                    C.c_void_p]),
     "nrpyell_relax_host": (C.c_int, [P(abi.paramstruct), XX, P(abi.bc_struct), P(abi.rfm_struct), PREAL, PREAL,
                                      C.c_double, C.c_double, C.c_int, C.c_double, P(C.c_int), P(C.c_double)]),
 }

@@ -19,7 +19,7 @@ INCLUDE = os.path.join(ROOT, "include")
 LIB = os.path.join(HERE, "libnrpyell_gpu.so")
 
 SOURCES = ["capi.cu", "driver.cu", "batch.cu", "tables.cu", "kernels_ref.cu", "kernels_fused.cu", "kernels_bulk.cu",
-           "noalloc.cu", "setup.cpp"]
+           "noalloc.cu", "mlp.cu", "setup.cpp"]
 OBJDIR = os.path.join(HERE, "_build")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 
@@ -43,8 +43,6 @@ def build(force=False, verbose=False):
     srcs = [os.path.join(CSRC, s) for s in SOURCES]
     headers = [os.path.join(CSRC, f) for f in os.listdir(CSRC) if f.endswith((".h", ".cuh"))]
     headers += [os.path.join(INCLUDE, f) for f in os.listdir(INCLUDE) if f.endswith(".h")]
-    if not force and not _stale(LIB, srcs + headers):
-        return LIB
     os.makedirs(OBJDIR, exist_ok=True)
     flags = ARCH + ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC,-fopenmp,-O3", "-I", INCLUDE, "-I", CSRC]
     jobs = []
@@ -60,6 +58,8 @@ def build(force=False, verbose=False):
     if failed:
         raise subprocess.CalledProcessError(1, failed[0])
     objs = [os.path.join(OBJDIR, os.path.basename(s) + ".o") for s in srcs]
+    if not jobs and not _stale(LIB, objs):
+        return LIB
     cmd = [nvcc()] + ARCH + ["-shared", "-Xlinker", "-Bsymbolic", "-o", LIB] + objs + ["-lgomp", "-lcudart"]
     if verbose:
         print(" ".join(cmd))

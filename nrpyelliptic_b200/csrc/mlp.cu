@@ -1,0 +1,453 @@
+// Learned initial guess: a small MLP (puncture parameters -> POD coefficients
+// of uu) trained and evaluated on the GPU with BF16 tensor-core matrix
+// products (mma.sync m16n8k16, FP32 accumulation), FP32 master weights and
+// Adam; plus the POD reconstruction of the guess.
+//
+// Every matrix product of the network -- forward Z = H W, backward
+// dH = dZ W^T and dW = H^T dZ -- is one kernel, k_gemm_bf16: 64x64 output
+// tiles, four warps of 32x32, operands read with arbitrary strides (so the
+// transposes are free), rounded to BF16 into shared memory and multiplied
+// with FP32 accumulators, with the bias and tanh of the forward pass fused
+// into the epilogue.
+#include <cuda_bf16.h>
+#include <math.h>
+#include <stdint.h>
+#include <string.h>
+
+#include <vector>
+
+#include "common.cuh"
+
+namespace nrpyell {
+
+namespace {
+
+// ------------------------------------------------------------------ GEMM
+// C[M x N] = alpha * A[M x K] B[K x N] (+ bias[N]) (then tanh), with
+// A(m,k) = A[m*sam + k*sak] and B(k,n) = B[k*sbk + n*sbn]; FP32 in and out.
+constexpr int GT = 64;  // output tile
+constexpr int GK = 16;  // k step (one mma)
+constexpr int EPI_NONE = 0, EPI_BIAS = 1, EPI_BIAS_TANH = 2;
+
+__device__ __forceinline__ uint32_t pack_bf16(float lo, float hi) {
+  const __nv_bfloat16 l = __float2bfloat16_rn(lo), h = __float2bfloat16_rn(hi);
+  return (uint32_t)__bfloat16_as_ushort(l) | ((uint32_t)__bfloat16_as_ushort(h) << 16);
+}
+
+__global__ void __launch_bounds__(128) k_gemm_bf16(int M, int N, int K, const float* __restrict__ A, long long sam,
+                                                  long long sak, const float* __restrict__ B, long long sbk,
+                                                  long long sbn, float* __restrict__ Cm, long long ldc,
+                                                  const float* __restrict__ bias, int epi, float alpha) {
+  // As[m][k/2], Bs[n][k/2]: BF16 pairs along k packed in 32 bits
+  __shared__ uint32_t As[GT][GK / 2 + 1];
+  __shared__ uint32_t Bs[GT][GK / 2 + 1];
+  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+  const int m0 = blockIdx.y * GT, n0 = blockIdx.x * GT;
+  const int wm = (warp >> 1) * 32, wn = (warp & 1) * 32;  // warp tile origin
+  const int g = lane >> 2, t = lane & 3;
+  float acc[2][4][4];
+#pragma unroll
+  for (int i = 0; i < 2; i++)
+#pragma unroll
+    for (int j = 0; j < 4; j++)
+#pragma unroll
+      for (int r = 0; r < 4; r++) acc[i][j][r] = 0.f;
+  for (int k0 = 0; k0 < K; k0 += GK) {
+    // 64 x 8 packed pairs per operand, 128 threads: 4 pairs each
+    for (int e = tid; e < GT * GK / 2; e += 128) {
+      const int r = e / (GK / 2), kp = e % (GK / 2);
+      const int k = k0 + 2 * kp;
+      const int m = m0 + r, n = n0 + r;
+      float a0 = 0.f, a1 = 0.f, b0 = 0.f, b1 = 0.f;
+      if (m < M) {
+        if (k < K) a0 = A[m * sam + k * sak];
+        if (k + 1 < K) a1 = A[m * sam + (k + 1) * sak];
+      }
+      if (n < N) {
+        if (k < K) b0 = B[k * sbk + n * sbn];
+        if (k + 1 < K) b1 = B[(k + 1) * sbk + n * sbn];
+      }
+      As[r][kp] = pack_bf16(a0, a1);
+      Bs[r][kp] = pack_bf16(b0, b1);
+    }
+    __syncthreads();
+    // fragments of mma.m16n8k16 (row A, col B): lane (g, t) holds A rows g
+    // and g+8 at k = 2t, 2t+1 and 2t+8, 2t+9, B column g at the same k
+    uint32_t af[2][4], bfr[4][2];
+#pragma unroll
+    for (int i = 0; i < 2; i++) {
+      const int r = wm + 16 * i + g;
+      af[i][0] = As[r][t];
+      af[i][1] = As[r + 8][t];
+      af[i][2] = As[r][t + 4];
+      af[i][3] = As[r + 8][t + 4];
+    }
+#pragma unroll
+    for (int j = 0; j < 4; j++) {
+      const int c = wn + 8 * j + g;
+      bfr[j][0] = Bs[c][t];
+      bfr[j][1] = Bs[c][t + 4];
+    }
+#pragma unroll
+    for (int i = 0; i < 2; i++)
+#pragma unroll
+      for (int j = 0; j < 4; j++)
+        asm volatile(
+            "mma.sync.aligned.m16n8k16.row.col.f32.bf16.bf16.f32 {%0,%1,%2,%3}, {%4,%5,%6,%7}, {%8,%9}, "
+            "{%0,%1,%2,%3};\n"
+            : "+f"(acc[i][j][0]), "+f"(acc[i][j][1]), "+f"(acc[i][j][2]), "+f"(acc[i][j][3])
+            : "r"(af[i][0]), "r"(af[i][1]), "r"(af[i][2]), "r"(af[i][3]), "r"(bfr[j][0]), "r"(bfr[j][1]));
+    __syncthreads();
+  }
+  // accumulator lane (g, t): rows g, g+8, columns 2t, 2t+1
+#pragma unroll
+  for (int i = 0; i < 2; i++)
+#pragma unroll
+    for (int j = 0; j < 4; j++)
+#pragma unroll
+      for (int r = 0; r < 4; r++) {
+        const int m = m0 + wm + 16 * i + g + (r >= 2 ? 8 : 0);
+        const int n = n0 + wn + 8 * j + 2 * t + (r & 1);
+        if (m < M && n < N) {
+          float v = alpha * acc[i][j][r];
+          if (epi != EPI_NONE) v += bias[n];
+          if (epi == EPI_BIAS_TANH) v = tanhf(v);
+          Cm[m * ldc + n] = v;
+        }
+      }
+}
+
+void gemm(int M, int N, int K, const float* A, long long sam, long long sak, const float* B, long long sbk,
+          long long sbn, float* C, long long ldc, const float* bias, int epi, float alpha = 1.f) {
+  dim3 grid((N + GT - 1) / GT, (M + GT - 1) / GT);
+  NRPYELL_LAUNCH(k_gemm_bf16, grid, 128, 0, M, N, K, A, sam, sak, B, sbk, sbn, C, ldc, bias, epi, alpha);
+}
+
+// ------------------------------------------------------ elementwise pieces
+// dZ = dH * (1 - H^2) (tanh layers), in place on dH.
+__global__ void k_tanh_back(float* dh, const float* __restrict__ h, long long n) {
+  const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < n) dh[i] *= 1.f - h[i] * h[i];
+}
+// db[n] = sum over rows of dZ[:, n].
+__global__ void k_colsum(const float* __restrict__ dz, int rows, int cols, float* db) {
+  const int n = blockIdx.x * blockDim.x + threadIdx.x;
+  if (n >= cols) return;
+  float s = 0.f;
+  for (int r = 0; r < rows; r++) s += dz[(long long)r * cols + n];
+  db[n] = s;
+}
+// dY = 2 (Y - T) * scale; adds the block's sum of (Y - T)^2 to *loss.
+__global__ void k_mse(const float* __restrict__ y, const float* __restrict__ tgt, long long n, float scale, float* dy,
+                      double* loss) {
+  __shared__ double sh[8];
+  const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  double l = 0.0;
+  if (i < n) {
+    const float d = y[i] - tgt[i];
+    dy[i] = 2.f * d * scale;
+    l = (double)d * d;
+  }
+  for (int o = 16; o > 0; o >>= 1) l += __shfl_down_sync(0xffffffffu, l, o);
+  if ((threadIdx.x & 31) == 0) sh[threadIdx.x >> 5] = l;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double s = 0.0;
+    for (int w = 0; w < (int)(blockDim.x >> 5); w++) s += sh[w];
+    atomicAdd(loss, s);
+  }
+}
+// Adam on FP32 master parameters.
+__global__ void k_adam(float* p, const float* __restrict__ gr, float* m, float* v, long long n, float lr, float b1,
+                       float b2, float eps, float c1, float c2) {
+  const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const float g = gr[i];
+  const float mi = b1 * m[i] + (1.f - b1) * g;
+  const float vi = b2 * v[i] + (1.f - b2) * g * g;
+  m[i] = mi;
+  v[i] = vi;
+  p[i] -= lr * (mi / c1) / (sqrtf(vi / c2) + eps);
+}
+// Rows of src selected by idx -> dst (minibatch gather).
+__global__ void k_gather_rows(const float* __restrict__ src, const int* __restrict__ idx, int rows, int cols,
+                              float* dst) {
+  const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= (long long)rows * cols) return;
+  const int r = (int)(i / cols), c = (int)(i % cols);
+  dst[i] = src[(long long)idx[r] * cols + c];
+}
+
+unsigned blocks_for(long long n, int bs) { return (unsigned)((n + bs - 1) / bs); }
+
+}  // namespace
+
+// ------------------------------------------------------------------- MLP
+
+struct Mlp {
+  int n_in, width, depth, n_out, batch_max;
+  // layer l: dims[l] -> dims[l+1]; W_l [in x out] row-major, then b_l
+  std::vector<int> dims;
+  std::vector<long long> woff, boff;  // offsets into the parameter vector
+  long long n_params = 0;
+  float *p = nullptr, *grad = nullptr, *m = nullptr, *v = nullptr;
+  std::vector<float*> h;  // output of layer l [batch_max x dims[l+1]]
+  float* x = nullptr;     // minibatch inputs
+  float* t = nullptr;     // minibatch targets
+  float* dbuf[2] = {nullptr, nullptr};
+  double* loss = nullptr;
+  int* idx = nullptr;
+  long long step = 0;
+};
+
+static Mlp* mlp_new(int n_in, int width, int depth, int n_out, int batch_max, unsigned seed) {
+  Mlp* q = new Mlp();
+  q->n_in = n_in;
+  q->width = width;
+  q->depth = depth;
+  q->n_out = n_out;
+  q->batch_max = batch_max;
+  q->dims.push_back(n_in);
+  for (int i = 0; i < depth; i++) q->dims.push_back(width);
+  q->dims.push_back(n_out);
+  const int L = (int)q->dims.size() - 1;
+  for (int l = 0; l < L; l++) {
+    q->woff.push_back(q->n_params);
+    q->n_params += (long long)q->dims[l] * q->dims[l + 1];
+    q->boff.push_back(q->n_params);
+    q->n_params += q->dims[l + 1];
+  }
+  // Glorot-uniform weights from a fixed 64-bit LCG, zero biases
+  std::vector<float> host(q->n_params, 0.f);
+  unsigned long long s = 0x9E3779B97F4A7C15ull ^ seed;
+  for (int l = 0; l < L; l++) {
+    const float a = sqrtf(6.f / (q->dims[l] + q->dims[l + 1]));
+    for (long long i = 0; i < (long long)q->dims[l] * q->dims[l + 1]; i++) {
+      s = s * 6364136223846793005ull + 1442695040888963407ull;
+      const float u = (float)((s >> 11) * (1.0 / 9007199254740992.0));
+      host[q->woff[l] + i] = a * (2.f * u - 1.f);
+    }
+  }
+  const size_t pb = sizeof(float) * q->n_params;
+  NRPYELL_CUDA(cudaMalloc(&q->p, pb));
+  NRPYELL_CUDA(cudaMalloc(&q->grad, pb));
+  NRPYELL_CUDA(cudaMalloc(&q->m, pb));
+  NRPYELL_CUDA(cudaMalloc(&q->v, pb));
+  NRPYELL_CUDA(cudaMemcpyAsync(q->p, host.data(), pb, cudaMemcpyHostToDevice, stream()));
+  NRPYELL_CUDA(cudaMemsetAsync(q->m, 0, pb, stream()));
+  NRPYELL_CUDA(cudaMemsetAsync(q->v, 0, pb, stream()));
+  int wmax = n_out > width ? n_out : width;
+  if (n_in > wmax) wmax = n_in;
+  for (int l = 0; l < L; l++) {
+    float* b = nullptr;
+    NRPYELL_CUDA(cudaMalloc(&b, sizeof(float) * (size_t)batch_max * q->dims[l + 1]));
+    q->h.push_back(b);
+  }
+  NRPYELL_CUDA(cudaMalloc(&q->x, sizeof(float) * (size_t)batch_max * n_in));
+  NRPYELL_CUDA(cudaMalloc(&q->t, sizeof(float) * (size_t)batch_max * n_out));
+  NRPYELL_CUDA(cudaMalloc(&q->dbuf[0], sizeof(float) * (size_t)batch_max * wmax));
+  NRPYELL_CUDA(cudaMalloc(&q->dbuf[1], sizeof(float) * (size_t)batch_max * wmax));
+  NRPYELL_CUDA(cudaMalloc(&q->loss, sizeof(double)));
+  NRPYELL_CUDA(cudaMalloc(&q->idx, sizeof(int) * batch_max));
+  NRPYELL_CUDA(cudaStreamSynchronize(stream()));
+  return q;
+}
+
+static void mlp_free(Mlp* q) {
+  if (!q) return;
+  cudaStreamSynchronize(stream());
+  cudaFree(q->p);
+  cudaFree(q->grad);
+  cudaFree(q->m);
+  cudaFree(q->v);
+  for (float* b : q->h) cudaFree(b);
+  cudaFree(q->x);
+  cudaFree(q->t);
+  cudaFree(q->dbuf[0]);
+  cudaFree(q->dbuf[1]);
+  cudaFree(q->loss);
+  cudaFree(q->idx);
+  delete q;
+}
+
+// Forward pass of `rows` inputs x [rows x n_in]; output in q->h.back().
+static void mlp_forward(Mlp* q, const float* x, int rows) {
+  const int L = (int)q->dims.size() - 1;
+  const float* in = x;
+  for (int l = 0; l < L; l++) {
+    const int K = q->dims[l], N = q->dims[l + 1];
+    gemm(rows, N, K, in, K, 1, q->p + q->woff[l], N, 1, q->h[l], N, q->p + q->boff[l],
+         l + 1 < L ? EPI_BIAS_TANH : EPI_BIAS);
+    in = q->h[l];
+  }
+}
+
+// Gradient of the mean squared error against t [rows x n_out] into q->grad
+// (after mlp_forward on the same x); adds the loss sum to *q->loss.
+static void mlp_backward(Mlp* q, const float* x, const float* t, int rows) {
+  const int L = (int)q->dims.size() - 1;
+  const long long nout = (long long)rows * q->n_out;
+  float* dz = q->dbuf[0];
+  NRPYELL_LAUNCH(k_mse, blocks_for(nout, 256), 256, 0, q->h[L - 1], t, nout, 1.f / (float)nout, dz, q->loss);
+  for (int l = L - 1; l >= 0; l--) {
+    const int K = q->dims[l], N = q->dims[l + 1];
+    const float* hin = (l == 0) ? x : q->h[l - 1];
+    // dW = hin^T dZ [K x N]: A(kk, r) = hin[r*K + kk], B(r, n) = dz[r*N + n]
+    gemm(K, N, rows, hin, 1, K, dz, N, 1, q->grad + q->woff[l], N, nullptr, EPI_NONE);
+    NRPYELL_LAUNCH(k_colsum, blocks_for(N, 128), 128, 0, dz, rows, N, q->grad + q->boff[l]);
+    if (l > 0) {
+      // dH_{l-1} = dZ W^T [rows x K]: B(n, kk) = W[kk*N + n]
+      float* dh = q->dbuf[(L - l) & 1];
+      gemm(rows, K, N, dz, N, 1, q->p + q->woff[l], 1, N, dh, K, nullptr, EPI_NONE);
+      NRPYELL_LAUNCH(k_tanh_back, blocks_for((long long)rows * K, 256), 256, 0, dh, q->h[l - 1], (long long)rows * K);
+      dz = dh;
+    }
+  }
+}
+
+static void mlp_adam(Mlp* q, float lr) {
+  const float b1 = 0.9f, b2 = 0.999f, eps = 1e-8f;
+  q->step++;
+  const float c1 = 1.f - powf(b1, (float)q->step), c2 = 1.f - powf(b2, (float)q->step);
+  NRPYELL_LAUNCH(k_adam, blocks_for(q->n_params, 256), 256, 0, q->p, q->grad, q->m, q->v, q->n_params, lr, b1, b2,
+                 eps, c1, c2);
+}
+
+// ------------------------------------------------------------ POD guess
+// y[0..Ntot) = mean + sum_k c[k] basis[k][.] (uu), y[Ntot..2 Ntot) = eta uu (vv).
+__global__ void k_pod_guess(const float* __restrict__ mean, const float* __restrict__ basis, int K, long long ntot,
+                            const float* __restrict__ c, double eta, double* y) {
+  extern __shared__ float cs[];
+  for (int k = threadIdx.x; k < K; k += blockDim.x) cs[k] = c[k];
+  __syncthreads();
+  const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= ntot) return;
+  double u = (double)mean[i];
+  for (int k = 0; k < K; k++) u += (double)cs[k] * (double)basis[(long long)k * ntot + i];
+  y[i] = u;
+  y[ntot + i] = eta * u;
+}
+
+}  // namespace nrpyell
+
+using namespace nrpyell;
+
+extern "C" {
+
+void* nrpyell_mlp_create(int n_in, int width, int depth, int n_out, int batch_max, unsigned seed) {
+  if (n_in <= 0 || width <= 0 || depth < 0 || n_out <= 0 || batch_max <= 0) {
+    NRPYELL_FAIL("nrpyell_mlp_create: sizes must be positive");
+    return nullptr;
+  }
+  Mlp* q = mlp_new(n_in, width, depth, n_out, batch_max, seed);
+  if (!status_ok()) {
+    mlp_free(q);
+    return nullptr;
+  }
+  return q;
+}
+
+void nrpyell_mlp_destroy(void* mlp) { mlp_free((Mlp*)mlp); }
+
+long long nrpyell_mlp_num_params(void* mlp) { return mlp ? ((Mlp*)mlp)->n_params : 0; }
+
+int nrpyell_mlp_get_params(void* mlp, float* host) {
+  Mlp* q = (Mlp*)mlp;
+  NRPYELL_CUDA(cudaMemcpyAsync(host, q->p, sizeof(float) * q->n_params, cudaMemcpyDeviceToHost, stream()));
+  NRPYELL_CUDA(cudaStreamSynchronize(stream()));
+  return status_ok() ? 0 : -1;
+}
+int nrpyell_mlp_set_params(void* mlp, const float* host) {
+  Mlp* q = (Mlp*)mlp;
+  NRPYELL_CUDA(cudaMemcpyAsync(q->p, host, sizeof(float) * q->n_params, cudaMemcpyHostToDevice, stream()));
+  NRPYELL_CUDA(cudaStreamSynchronize(stream()));
+  return status_ok() ? 0 : -1;
+}
+
+int nrpyell_mlp_predict(void* mlp, const float* x, int n, float* y) {
+  Mlp* q = (Mlp*)mlp;
+  for (int r0 = 0; r0 < n; r0 += q->batch_max) {
+    const int rows = (n - r0 < q->batch_max) ? n - r0 : q->batch_max;
+    mlp_forward(q, x + (long long)r0 * q->n_in, rows);
+    NRPYELL_CUDA(cudaMemcpyAsync(y + (long long)r0 * q->n_out, q->h.back(), sizeof(float) * rows * q->n_out,
+                                 cudaMemcpyDeviceToDevice, stream()));
+  }
+  NRPYELL_CUDA(cudaStreamSynchronize(stream()));
+  return status_ok() ? 0 : -1;
+}
+
+double nrpyell_mlp_loss_grad(void* mlp, const float* x, const float* t, int rows, float* grad_host) {
+  Mlp* q = (Mlp*)mlp;
+  if (rows > q->batch_max || rows <= 0) {
+    NRPYELL_FAIL("nrpyell_mlp_loss_grad: need 0 < rows <= batch_max");
+    return NAN;
+  }
+  NRPYELL_CUDA(cudaMemsetAsync(q->loss, 0, sizeof(double), stream()));
+  mlp_forward(q, x, rows);
+  mlp_backward(q, x, t, rows);
+  double loss = NAN;
+  NRPYELL_CUDA(cudaMemcpyAsync(&loss, q->loss, sizeof(double), cudaMemcpyDeviceToHost, stream()));
+  if (grad_host)
+    NRPYELL_CUDA(cudaMemcpyAsync(grad_host, q->grad, sizeof(float) * q->n_params, cudaMemcpyDeviceToHost, stream()));
+  NRPYELL_CUDA(cudaStreamSynchronize(stream()));
+  return loss / ((double)rows * q->n_out);
+}
+
+double nrpyell_mlp_train(void* mlp, const float* x, const float* t, int n, int batch, int epochs, float lr,
+                         unsigned seed, double* loss_history) {
+  Mlp* q = (Mlp*)mlp;
+  if (batch > q->batch_max || batch <= 0 || n < batch || epochs < 1) {
+    NRPYELL_FAIL("nrpyell_mlp_train: need 0 < batch <= batch_max, batch <= n and epochs >= 1");
+    return NAN;
+  }
+  std::vector<int> perm(n);
+  for (int i = 0; i < n; i++) perm[i] = i;
+  unsigned long long s = 0xD1B54A32D192ED03ull ^ seed;
+  const int per_epoch = n / batch;
+  const long long total = (long long)per_epoch * epochs;
+  long long it = 0;
+  double last = NAN;
+  for (int e = 0; e < epochs && status_ok(); e++) {
+    // the previous epoch's index copies read perm: let them finish first
+    NRPYELL_CUDA(cudaStreamSynchronize(stream()));
+    for (int i = n - 1; i > 0; i--) {  // Fisher-Yates
+      s = s * 6364136223846793005ull + 1442695040888963407ull;
+      const int j = (int)((s >> 33) % (unsigned long long)(i + 1));
+      const int tmp = perm[i];
+      perm[i] = perm[j];
+      perm[j] = tmp;
+    }
+    NRPYELL_CUDA(cudaMemsetAsync(q->loss, 0, sizeof(double), stream()));
+    for (int b = 0; b < per_epoch; b++, it++) {
+      NRPYELL_CUDA(cudaMemcpyAsync(q->idx, perm.data() + (long long)b * batch, sizeof(int) * batch,
+                                   cudaMemcpyHostToDevice, stream()));
+      NRPYELL_LAUNCH(k_gather_rows, blocks_for((long long)batch * q->n_in, 256), 256, 0, x, q->idx, batch, q->n_in,
+                     q->x);
+      NRPYELL_LAUNCH(k_gather_rows, blocks_for((long long)batch * q->n_out, 256), 256, 0, t, q->idx, batch,
+                     q->n_out, q->t);
+      mlp_forward(q, q->x, batch);
+      mlp_backward(q, q->x, q->t, batch);
+      const float lr_t = lr * (0.01f + 0.99f * 0.5f * (1.f + cosf(3.14159265f * (float)it / (float)total)));
+      mlp_adam(q, lr_t);
+    }
+    double sum = 0.0;
+    NRPYELL_CUDA(cudaMemcpyAsync(&sum, q->loss, sizeof(double), cudaMemcpyDeviceToHost, stream()));
+    NRPYELL_CUDA(cudaStreamSynchronize(stream()));
+    last = sum / ((double)per_epoch * batch * q->n_out);
+    if (loss_history) loss_history[e] = last;
+  }
+  return last;
+}
+
+int nrpyell_pod_guess(const float* mean, const float* basis, int K, long long ntot, const float* c, double eta,
+                      double* y_n) {
+  if (K <= 0 || K > 4096 || ntot <= 0) {
+    NRPYELL_FAIL("nrpyell_pod_guess: need 0 < K <= 4096 and ntot > 0");
+    return -1;
+  }
+  NRPYELL_LAUNCH(k_pod_guess, blocks_for(ntot, 256), 256, sizeof(float) * K, mean, basis, K, ntot, c, eta, y_n);
+  NRPYELL_CUDA(cudaStreamSynchronize(stream()));
+  return status_ok() ? 0 : -1;
+}
+
+}  // extern "C"

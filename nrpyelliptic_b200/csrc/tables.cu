@@ -80,7 +80,8 @@ RfmTables* get_rfm_tables(const paramstruct* p, const rfm_struct* rfm) {
   const Dims d = dims_of(p);
   for (RfmTables* t : g_rfm)
     if (t->key_f0 == rfm->f0_of_xx0 && t->key_f2 == rfm->f2_of_xx0_xx1 && same_dims(t->d, d) &&
-        t->invdx[0] == p->invdx0 && t->invdx[1] == p->invdx1 && t->invdx[2] == p->invdx2)
+        t->invdx[0] == p->invdx0 && t->invdx[1] == p->invdx1 && t->invdx[2] == p->invdx2 && t->AMAX == p->AMAX &&
+        t->SINHWAA == p->SINHWAA && t->bScale == p->bScale)
       return t;
   if (!rfm->f0_of_xx0 || !rfm->f2_of_xx0_xx1 || !rfm->f1_of_xx1 || !rfm->f3_of_xx0) {
     NRPYELL_FAIL("rfm_struct has NULL arrays (call rfm_precompute_rfmstruct_define first)");
@@ -93,6 +94,9 @@ RfmTables* get_rfm_tables(const paramstruct* p, const rfm_struct* rfm) {
   t->invdx[0] = p->invdx0;
   t->invdx[1] = p->invdx1;
   t->invdx[2] = p->invdx2;
+  t->AMAX = p->AMAX;
+  t->SINHWAA = p->SINHWAA;
+  t->bScale = p->bScale;
   const size_t n0 = d.N0, n1 = d.N1, n01 = n0 * n1;
   const size_t n_doubles = 5 * n0 + 2 * n1 + 2 * n01 + kNumCoef * n01;
   const size_t bytes = n_doubles * sizeof(double) + kNumCoef * n01 * sizeof(float) + 256;

@@ -21,6 +21,7 @@ struct RfmTables {
   const REAL* key_f2;
   Dims d;
   double invdx[3];
+  double AMAX, SINHWAA, bScale;  // the content depends on these (host arrays may be reused)
   // device copies of the reference-metric arrays
   double* f0;
   double* f0_D0;
