@@ -261,6 +261,33 @@ def run_ours(args, dist):
     ms_max = dist.max(ms)
     value = dist.world * args.steps / (ms_max * 1e-3)
 
+    # The same workload through the FP32-then-FP64 driver: FP32 storage and
+    # arithmetic until log10 L2 <= -7 (or a stall), then FP64 to -10; the
+    # solution's error is taken against the FP64 solve's.
+    u64 = ds.download("y_n")
+    n32, n64 = C.c_int(0), C.c_int(0)
+
+    def solve_mixed():
+        lib.nrpyell_memset(ds.ptr["y_n"], 0, n2)
+        lib.nrpyell_flush_l2()
+        rc = lib.nrpyell_relax_mixed(C.byref(ds.g), prob.dt, TOL, -7.0, 1000, 0.98, args.max_steps, cfg.R_L2,
+                                     C.byref(n32), C.byref(n64), C.byref(fin), None)
+        _lib.check(lib)
+        if rc != 0:
+            raise RuntimeError("mixed-precision solve did not converge")
+
+    solve_mixed()
+    dist.barrier()
+    lib.nrpyell_event_record(4)
+    for _ in range(args.steps):
+        solve_mixed()
+    lib.nrpyell_event_record(5)
+    ms_mixed = dist.max(lib.nrpyell_event_elapsed_ms(4, 5))
+    um = ds.download("y_n")
+    mixed = {"value": dist.world * args.steps / (ms_mixed * 1e-3), "unit": "solves/s",
+             "fp32_steps": n32.value, "fp64_steps": n64.value, "switch_log10_l2": -7.0,
+             "max_rel_err_vs_fp64": float(np.max(np.abs(um - u64)) / np.max(np.abs(u64)))}
+
     # End to end through the host-buffer entry point: H2D of the auxevol
     # gridfunctions and the initial guess, the solve, D2H of the solution.
     aux_h = lib.nrpyell_host_pinned_malloc(abi.NUM_AUXEVOL_GFS * prob.Ntot * 8)
@@ -334,7 +361,7 @@ def run_ours(args, dist):
             "e2e": {"value": e2e, "unit": "solves/s", "h2d_bytes_per_step": (abi.NUM_AUXEVOL_GFS + 2) * prob.Ntot * 8,
                     "d2h_bytes_per_step": n2},
             "gpu_launches": int(launches), "clocks": clk, "roofline": roofline,
-            "roofline_out_of_l2": roofline_big}
+            "roofline_out_of_l2": roofline_big, "mixed_precision": mixed}
     ds.free()
     if dist.rank == 0 and dist.world == 1 and not args.no_cpu_baseline:
         t_it, kind, cores, n = cpu_time_per_iteration(cfg, args.cpu_seconds)

@@ -169,6 +169,13 @@ void nrpyell_auxevol_gfs_all_points(const paramstruct *params, REAL *xx[3], REAL
 void nrpyell_wavespeed_gf_all_points(const paramstruct *params, const REAL CFL_FACTOR, const REAL dt, REAL *xx[3],
                                      REAL *auxevol_gfs);                                                /* wavespeed_gf_all_points.c */
 REAL nrpyell_compute_wavespeed_at_OB(const paramstruct *params, const REAL *auxevol_gfs);               /* compute_wavespeed_at_OB.c */
+/* The three auxevol gridfunctions computed on the GPU straight into device
+ * memory (auxevol_gfs: 3 Ntot doubles): psi_background and ADD_times_AUU at
+ * all points, the wavespeed CFL_FACTOR * min(ds) / dt on the interior and 0
+ * in the ghost zones -- the nrpyell_auxevol_gfs_all_points and
+ * nrpyell_wavespeed_gf_all_points results without host arrays or copies. */
+int nrpyell_auxevol_device(const paramstruct *params, REAL *xx[3], const REAL CFL_FACTOR, const REAL dt,
+                           REAL *auxevol_gfs);
 
 /* Stop-on-tolerance relaxation on device-resident gridfunctions.
  * For n = 0, 1, ..., max_steps: evaluate the residual of y_n and its L2 norm
@@ -196,6 +203,33 @@ int nrpyell_relax_mixed(griddata_struct *griddata, const REAL dt, const REAL log
                         const REAL integration_radius, int *steps_fp32, int *steps_fp64, REAL *final_log10_l2,
                         REAL *history);
 
+/* The same relaxation with the stopping rule of the Einstein Toolkit thorn
+ * (NRPyEllipticET_conformally_flat_BBH_Hyperbolic_Relaxation.c:185-217):
+ * its loop n = 0..max_iterations takes one RK4 step, then, when n is a
+ * multiple of check_every or n == max_iterations, evaluates the residual of
+ * the new state and stops once log10 L2 < log_target_residual (strictly).
+ * *iterations = the n of the last test; returns 0 when the target was met, 1
+ * when it was not (the thorn errors out there), < 0 on error. */
+int nrpyell_relax_et(griddata_struct *griddata, const REAL dt, const REAL log_target_residual, const int max_iterations,
+                     const int check_every, const REAL integration_radius, int *iterations, REAL *final_log10_l2);
+/* Damping parameter of arXiv:2111.02424 (the thorn's
+ * conformally_flat_BBH_set_optimum_eta_damping.c:3-27): TRC from Eq. (B6),
+ * eta = 6.9 TRC^-0.79 - 0.7 from Eq. (36), fitted for AMAX = 1e6,
+ * SINHWAA = 0.07 and bScale = 5; writes params->eta_damping. */
+REAL nrpyell_compute_TRC(const REAL A, const REAL b, const REAL C_0, const REAL dt, const REAL dxx1, const REAL dxx2);
+void nrpyell_set_optimum_eta_damping(const REAL dt, const REAL CFL_FACTOR, paramstruct *params);
+/* Solution export (the Einstein Toolkit thorn's Initialize_ADMBase role,
+ * without Cactus): for npts Cartesian points xyz (host, x y z per point, in
+ * this code's frame), uu by Lagrange interpolation of the given order (1..8;
+ * the thorn's default is 4) on the (xx0,xx1,xx2) grid including ghost zones
+ * from uu (device: the uu gridfunction of a y_n whose ghost zones are
+ * filled, as the relaxation drivers leave it), and the ADM quantities of the
+ * conformally flat data: psi = psi_background + uu, gamma_ij = psi^4
+ * delta_ij, K_ij = psi^-2 Abar_ij (Bowen-York; beta = 0).  Outputs (host,
+ * each optional): uu_out, psi_out [npts]; gamma_out, K_out [6 npts] in the
+ * order xx xy xz yy yz zz. */
+int nrpyell_interpolate_solution(const paramstruct *params, REAL *xx[3], const REAL *uu, int npts, const REAL *xyz,
+                                 int order, REAL *uu_out, REAL *psi_out, REAL *gamma_out, REAL *K_out);
 /* Batched relaxation: n configurations, each a griddata_struct set up as for
  * nrpyell_relax (its own grid size, parameters, bc_struct, rfm_struct and
  * device gridfunctions; dt[c] its time step), relaxed together from their

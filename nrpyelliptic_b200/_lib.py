@@ -72,11 +72,18 @@ EXPORTS = {
     "nrpyell_auxevol_gfs_all_points": (None, [P(abi.paramstruct), XX, PREAL]),
     "nrpyell_wavespeed_gf_all_points": (None, [P(abi.paramstruct), C.c_double, C.c_double, XX, PREAL]),
     "nrpyell_compute_wavespeed_at_OB": (C.c_double, [P(abi.paramstruct), PREAL]),
+    "nrpyell_auxevol_device": (C.c_int, [P(abi.paramstruct), XX, C.c_double, C.c_double, PREAL]),
     "nrpyell_relax": (C.c_int, [P(abi.griddata_struct), C.c_double, C.c_double, C.c_int, C.c_double, P(C.c_int),
                                 P(C.c_double), PREAL]),
     "nrpyell_relax_mixed": (C.c_int, [P(abi.griddata_struct), C.c_double, C.c_double, C.c_double, C.c_int,
                                       C.c_double, C.c_int, C.c_double, P(C.c_int), P(C.c_int), P(C.c_double),
                                       PREAL]),
+    "nrpyell_relax_et": (C.c_int, [P(abi.griddata_struct), C.c_double, C.c_double, C.c_int, C.c_int, C.c_double,
+                                   P(C.c_int), P(C.c_double)]),
+    "nrpyell_compute_TRC": (C.c_double, [C.c_double] * 6),
+    "nrpyell_set_optimum_eta_damping": (None, [C.c_double, C.c_double, P(abi.paramstruct)]),
+    "nrpyell_interpolate_solution": (C.c_int, [P(abi.paramstruct), XX, PREAL, C.c_int, PREAL, C.c_int, PREAL, PREAL,
+                                               PREAL, PREAL]),
     "nrpyell_relax_batch": (C.c_int, [C.c_int, P(abi.griddata_struct), PREAL, C.c_double, C.c_int, C.c_double,
                                       P(C.c_int), PREAL]),
     "nrpyell_mlp_create": (C.c_void_p, [C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, C.c_uint]),

@@ -530,6 +530,46 @@ int nrpyell_relax(griddata_struct* g, const REAL dt, const REAL log10_tol, const
   return r.converged ? 0 : 1;
 }
 
+int nrpyell_relax_et(griddata_struct* g, const REAL dt, const REAL log_target_residual, const int max_iterations,
+                     const int check_every, const REAL integration_radius, int* iterations, REAL* final_log10_l2) {
+  if (check_every < 1 || max_iterations < 0) {
+    NRPYELL_FAIL("nrpyell_relax_et: need check_every >= 1 and max_iterations >= 0");
+    return -1;
+  }
+  RelaxSetup su;
+  // the thorn's loop takes up to max_iterations + 1 steps and tests after each
+  const int rc = relax_prepare(g, max_iterations + 1, integration_radius, &su, "nrpyell_relax_et");
+  if (rc) return rc;
+  const StateBuffers b = buffers_of(&g->gridfuncs);
+  RelaxParams rp = relax_params(&g->params, dt);
+  rp.log10_tol = log_target_residual;
+  rp.max_steps = max_iterations + 1;
+  rp.check_every = check_every;
+  const int tile = tuned_tile<double>(su.d, su.rt, su.bt, su.w, su.s, b, rp);
+  const RelaxResult r = relax_loop<double>(su.d, su.rt, su.bt, su.lt, su.w, su.s, tile, b, rp);
+  launch_ghost_fill<double>(su.d, su.bt, g->gridfuncs.y_n_gfs);
+  NRPYELL_CUDA(cudaStreamSynchronize(stream()));
+  if (!status_ok()) return -1;
+  // r.steps RK4 steps were taken before the last residual: the thorn's
+  // loop index at that test is r.steps - 1
+  if (iterations) *iterations = r.steps - 1;
+  if (final_log10_l2) *final_log10_l2 = r.last_log10_l2;
+  return r.converged ? 0 : 1;
+}
+
+REAL nrpyell_compute_TRC(const REAL A, const REAL b, const REAL C_0, const REAL dt, const REAL dxx1,
+                         const REAL dxx2) {
+  // Eq. (B6) of arXiv:2111.02424 in this code's coordinate names
+  const double c1 = cos(dxx1 / 2.0), c2 = cos(dxx2 / 2.0);
+  return dt / (C_0 * dxx1) * atanh(A / sqrt(A * A + b * b * c1 * c1)) * c1 * c2;
+}
+
+void nrpyell_set_optimum_eta_damping(const REAL dt, const REAL CFL_FACTOR, paramstruct* params) {
+  // Eq. (36) of arXiv:2111.02424: eta = 6.9 TRC^-0.79 - 0.7
+  const double trc = nrpyell_compute_TRC(params->AMAX, params->bScale, CFL_FACTOR, dt, params->dxx1, params->dxx2);
+  params->eta_damping = 6.9 * pow(trc, -0.79) - 0.7;
+}
+
 int nrpyell_relax_mixed(griddata_struct* g, const REAL dt, const REAL log10_tol, const REAL log10_switch,
                         const int stall_window, const REAL stall_factor, const int max_steps,
                         const REAL integration_radius, int* steps_fp32, int* steps_fp64, REAL* final_log10_l2,

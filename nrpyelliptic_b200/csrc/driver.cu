@@ -104,6 +104,7 @@ SubstepArgs substep_args(const Dims& d, RfmTables* rt, BcTables* bt, Scratch* s,
   a.history = nullptr;
   a.log10_tol = -1e300;
   a.max_steps = 0;
+  a.check_every = 0;
   a.stall = nullptr;
   a.stall_window = 0;
   a.stall_log_drop = 0.0;
@@ -218,6 +219,7 @@ RelaxResult relax_loop(const Dims& d, RfmTables* rt, BcTables* bt, L2Tables* lt,
       a1.history = w->history + rp.history_offset;
       a1.log10_tol = rp.log10_tol;
       a1.max_steps = rp.max_steps;
+      a1.check_every = rp.check_every;
       a1.stall = w->stall;
       a1.stall_window = rp.stall_window;
       a1.stall_log_drop = rp.stall_log_drop;

@@ -34,6 +34,7 @@ struct RelaxParams {
   double dt, eta, cOB[2];
   double log10_tol;
   int max_steps;
+  int check_every;  // 0: stop test on every residual (main.c); > 0: ET thorn semantics
   int stall_window;       // 0: no stall test
   double stall_log_drop;  // stalled when log10 L2 fell by less than this over the window (negative)
   int history_offset;     // history index of step 0 of this run

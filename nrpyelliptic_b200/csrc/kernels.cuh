@@ -41,6 +41,7 @@ struct SubstepArgs {
   double* history;
   double log10_tol;
   int max_steps;
+  int check_every;  // 0: test every residual (main.c); > 0: the ET thorn's loop
   // Optional stall test: stop (state[3] = 1) once the best log10 L2 so far
   // has not dropped by at least -stall_log_drop for stall_window steps;
   // stall[0..1] = best log10 L2 and the step it was reached.

@@ -237,6 +237,47 @@ __global__ void __launch_bounds__(128) k_radiation_rows(SubDev<T> a) {
 // reads at compile-time offsets and the per-point integer work is small.
 // uu along i2 stays in registers and the pointwise inputs of all P planes are
 // loaded before the first store.
+// Copies uu on plane i2 of an interior tile, widened by 5 points along i0
+// and i1 (rows i10-5 .. i10+BY+4, points i00-5 .. i00+36), into su, one row
+// per warp iteration; ghost points are redirected to their sources only in
+// tiles that touch an inner boundary (`inner`).
+template <typename T, int BY>
+__device__ __forceinline__ void stage_plane(const SubDev<T>& a, const T* __restrict__ u, int i00, int i10, int i2,
+                                            bool inner, T (*su)[42]) {
+  constexpr int RWS = 42, NR = BY + 10;
+  const int tx = threadIdx.x & 31, ty = threadIdx.x >> 5;
+  const int N0 = a.N0, top = NGHOSTS + a.Nxx1;
+  const int N01 = (int)a.N01;
+  for (int r = ty; r < NR; r += BY) {
+    const int i1 = i10 - NGHOSTS + r;
+    if (i1 >= top + NGHOSTS) continue;  // never read
+    if (!inner) {
+      const T* src = u + (i00 - NGHOSTS) + N0 * i1 + N01 * i2;
+      su[r][tx] = __ldg(src + tx);
+      if (tx < RWS - 32 && i00 - NGHOSTS + 32 + tx < N0) su[r][32 + tx] = __ldg(src + 32 + tx);
+    } else {
+      for (int x = tx; x < RWS; x += 32) {
+        int j0 = i00 - NGHOSTS + x, j1 = i1;
+        if (j0 >= N0) continue;
+        bool flip = false;
+        if (j1 < NGHOSTS) {
+          j1 = 2 * NGHOSTS - 1 - j1;
+          flip = true;
+        } else if (j1 >= top) {
+          j1 = 2 * top - 1 - j1;
+          flip = true;
+        }
+        if (j0 < NGHOSTS) {
+          j0 = 2 * NGHOSTS - 1 - j0;
+          flip = !flip;
+        }
+        const int j2 = flip ? wrap2(i2 + a.half2, a.Nxx2) : i2;
+        su[r][x] = __ldg(u + j0 + N0 * j1 + N01 * j2);
+      }
+    }
+  }
+}
+
 // Shared memory of the planes kernel, in doubles: the planes of an interior
 // block, or the rows of a column block.
 template <typename T, int BY, int P>
@@ -264,37 +305,10 @@ __device__ __forceinline__ void planes_block(const SubDev<T>& a, int bid, double
   const int N0 = a.N0, top = NGHOSTS + a.Nxx1, zend = NGHOSTS + a.Nxx2;
   const int N01 = (int)a.N01;
   const T* __restrict__ u = a.S;
-  // ---- stage the planes, one row per warp iteration
+  // ---- stage the planes
   const bool inner = (t0 == 0) || (i10 < 2 * NGHOSTS) || (i10 + BY + NGHOSTS > top);
-  for (int row = ty; row < P * NR; row += BY) {
-    const int r = row % NR, p = row / NR;
-    const int i1 = i10 - NGHOSTS + r, i2 = z0 + p;
-    if (i2 >= zend || i1 >= top + NGHOSTS) continue;  // never read
-    if (!inner) {
-      const T* src = u + (i00 - NGHOSTS) + N0 * i1 + N01 * i2;
-      su[p][r][tx] = __ldg(src + tx);
-      if (tx < RWS - 32 && i00 - NGHOSTS + 32 + tx < N0) su[p][r][32 + tx] = __ldg(src + 32 + tx);
-    } else {
-      for (int x = tx; x < RWS; x += 32) {
-        int j0 = i00 - NGHOSTS + x, j1 = i1;
-        if (j0 >= N0) continue;
-        bool flip = false;
-        if (j1 < NGHOSTS) {
-          j1 = 2 * NGHOSTS - 1 - j1;
-          flip = true;
-        } else if (j1 >= top) {
-          j1 = 2 * top - 1 - j1;
-          flip = true;
-        }
-        if (j0 < NGHOSTS) {
-          j0 = 2 * NGHOSTS - 1 - j0;
-          flip = !flip;
-        }
-        const int j2 = flip ? wrap2(i2 + a.half2, a.Nxx2) : i2;
-        su[p][r][x] = __ldg(u + j0 + N0 * j1 + N01 * j2);
-      }
-    }
-  }
+  for (int p = 0; p < P; p++)
+    if (z0 + p < zend) stage_plane<T, BY>(a, u, i00, i10, z0 + p, inner, su[p]);
   const int i0 = i00 + tx, i1 = i10 + ty;
   const bool valid = i0 < NGHOSTS + a.Nxx0 && i1 < top;
   const int k2 = i0 + N0 * i1;

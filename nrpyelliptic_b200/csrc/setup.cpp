@@ -11,6 +11,8 @@
 #include <stdlib.h>
 #include <string.h>
 
+#include <vector>
+
 #include "nrpyell_gpu.h"
 #include "sinhsymtp.h"
 
@@ -275,20 +277,29 @@ void nrpyell_bcstruct_set_up(const paramstruct *p, bc_struct *bc) {
            i2 < N2 - NGHOSTS;
   };
 
-  // Step 1: inner points, in the reference's loop order (i2 outer, i0 inner).
-  int num_inner = 0;
-  for (int i2 = 0; i2 < N2; i2++)
+  // Step 1: inner points, in the reference's loop order (i2 outer, i0
+  // inner).  Counted per i2 plane, then written plane by plane in parallel
+  // from the planes' prefix offsets, which keeps that order.
+  std::vector<int> plane_count(N2, 0), plane_start(N2 + 1, 0);
+#pragma omp parallel for
+  for (int i2 = 0; i2 < N2; i2++) {
+    int c = 0;
     for (int i1 = 0; i1 < N1; i1++)
       for (int i0 = 0; i0 < N0; i0++) {
         if (interior(i0, i1, i2)) continue;
         int m[3];
         map_point(i0, i1, i2, m);
-        if (!(m[0] == i0 && m[1] == i1 && m[2] == i2)) num_inner++;
+        if (!(m[0] == i0 && m[1] == i1 && m[2] == i2)) c++;
       }
+    plane_count[i2] = c;
+  }
+  for (int i2 = 0; i2 < N2; i2++) plane_start[i2 + 1] = plane_start[i2] + plane_count[i2];
+  const int num_inner = plane_start[N2];
   bc->bc_info.num_inner_boundary_points = num_inner;
   bc->inner_bc_array = (innerpt_bc_struct *)malloc(sizeof(innerpt_bc_struct) * (num_inner > 0 ? num_inner : 1));
-  int w = 0;
-  for (int i2 = 0; i2 < N2; i2++)
+#pragma omp parallel for
+  for (int i2 = 0; i2 < N2; i2++) {
+    int w = plane_start[i2];
     for (int i1 = 0; i1 < N1; i1++)
       for (int i0 = 0; i0 < N0; i0++) {
         if (interior(i0, i1, i2)) continue;
@@ -303,6 +314,7 @@ void nrpyell_bcstruct_set_up(const paramstruct *p, bc_struct *bc) {
         const REAL par[10] = {1, d[0], d[1], d[2], d[0] * d[0], d[0] * d[1], d[0] * d[2], d[1] * d[1], d[1] * d[2], d[2] * d[2]};
         for (int t = 0; t < 10; t++) e.parity[t] = (par[t] < 0) ? -1 : 1;
       }
+  }
 
   // Step 2: pure outer points, grown layer by layer: x0 faces, then x1, then x2
   // (bcstruct_set_up.c:404-518).

@@ -36,6 +36,7 @@ struct SubDev {
   const int* done;
   double volume, log10_tol;
   int max_steps;
+  int check_every;  // > 0: Einstein Toolkit thorn semantics (see finalize_l2)
   double* stall;
   int stall_window;
   double stall_log_drop;
@@ -197,7 +198,14 @@ __device__ void finalize_l2(const SubDev<T>& a, double* sh) {
         stalled = true;
       }
     }
-    if (l2 <= a.log10_tol) {
+    // main.c semantics: the stop test on every residual, log10 L2 <= tol.
+    // The ET thorn's (NRPyEllipticET_..._Hyperbolic_Relaxation.c:185-217):
+    // its loop index counts steps already taken minus one, it tests after
+    // every check_every-th step and after the last one, with log10 L2 < tol.
+    bool test = true;
+    if (a.check_every > 0) test = n >= 1 && ((n - 1) % a.check_every == 0 || n >= a.max_steps);
+    const bool met = test && (a.check_every > 0 ? l2 < a.log10_tol : l2 <= a.log10_tol);
+    if (met) {
       a.state[2] = 1;
       a.state[1] = 1;
     } else if (stalled) {
@@ -420,6 +428,7 @@ inline SubDev<T> make_dev(const SubstepArgs& a, int by, int p) {
   f.volume = a.lt ? a.lt->volume : 1.0;
   f.log10_tol = a.log10_tol;
   f.max_steps = a.max_steps;
+  f.check_every = a.check_every;
   f.stall = a.stall;
   f.stall_window = a.stall_window;
   f.stall_log_drop = a.stall_log_drop;

@@ -15,7 +15,8 @@ Pipeline (one GPU):
      centred uu snapshots, float64 eigendecomposition), `--modes` modes;
   3. MLP 13 -> 4 x 512 (tanh) -> modes, trained with the library's BF16
      tensor-core kernels (nrpyell_mlp_train: Adam, minibatch 256) on
-     standardised inputs and per-mode standardised coefficients;
+     standardised inputs and the coefficients divided by their overall
+     standard deviation;
   4. held-out evaluation on `--test` configurations from another seed: RK4
      steps and wall time to log10 L2 <= -10 from the zero guess and from the
      learned guess (FP64, and FP32-then-FP64), the fallback rate, the guess's
@@ -50,7 +51,7 @@ def solve_snapshots(cfgs, lib, chunk=64, tol=-10.0, max_steps=40000, log=print):
     converged uu arrays (float32, ghost zones included) and step counts."""
     snaps, steps = None, []
     for c0 in range(0, len(cfgs), chunk):
-        probs = [Problem(c, lib=lib) for c in cfgs[c0:c0 + chunk]]
+        probs = [Problem(c, lib=lib, host_aux=False) for c in cfgs[c0:c0 + chunk]]
         rc, st, _, states = relax_batch(probs, tol=tol, max_steps=max_steps, lib=lib)
         if snaps is None:
             snaps = np.empty((len(cfgs), probs[0].Ntot), np.float32)
@@ -88,7 +89,10 @@ class Guess:
         self.lib = lib
         self.K, self.ntot = basis.shape
         self.fmu, self.fsd = feats.mean(0), feats.std(0) + 1e-12
-        self.csd = coeffs.std(0) + 1e-30
+        # one scale for all coefficients, so that the training loss is the
+        # squared L2 error of the reconstructed uu (standardising each mode
+        # would weight the barely-excited high modes like the leading ones)
+        self.csd = float(coeffs.std()) + 1e-30
         self.mlp = lib.nrpyell_mlp_create(N_FEATURES, width, depth, self.K, 256, seed)
         _lib.check(lib)
         self.d_mean = self._upload(mean)
@@ -176,7 +180,7 @@ def evaluate(lib, guess, cfgs, log=print):
     rows, zeros = [], []
     coeffs = guess.predict([features(c) for c in cfgs])
     for i, cfg in enumerate(cfgs):
-        prob = Problem(cfg, lib=lib)
+        prob = Problem(cfg, lib=lib, host_aux=False)
         ds = DeviceState(prob, lib=lib)
         r0 = initial_log10_l2(lib, prob, ds)
         s0, t0, f0 = timed_relax(lib, prob, ds, False)
@@ -263,7 +267,7 @@ def main():
     t = time.perf_counter()
     last, hist = guess.train(feats, coeffs, args.epochs)
     T["MLP training"] = time.perf_counter() - t
-    print("MLP training: %d epochs, loss (standardised coefficients) %.3e -> %.3e" % (args.epochs, hist[0], last))
+    print("MLP training: %d epochs, loss (scaled coefficients) %.3e -> %.3e" % (args.epochs, hist[0], last))
     test_cfgs = configs(args.test, args.test_seed)
     t = time.perf_counter()
     ev = evaluate(lib, guess, test_cfgs)

@@ -118,7 +118,7 @@ class Problem:
     auxevol gridfunctions and dt.  Arrays are numpy views of C memory owned
     by this object (freed in close())."""
 
-    def __init__(self, cfg, lib=None):
+    def __init__(self, cfg, lib=None, host_aux=True):
         self.cfg = cfg
         self.lib = lib = lib or _lib.load()
         p = abi.paramstruct()
@@ -136,13 +136,26 @@ class Problem:
         lib.nrpyell_rfm_precompute_rfmstruct_define(C.byref(p), self.xx, C.byref(self.rfm))
         self.N = (p.Nxx_plus_2NGHOSTS0, p.Nxx_plus_2NGHOSTS1, p.Nxx_plus_2NGHOSTS2)
         self.Ntot = self.N[0] * self.N[1] * self.N[2]
+        self._closed = False
+        if not host_aux:
+            # the auxevol gridfunctions are computed on the GPU by DeviceState
+            # (nrpyell_auxevol_device), which also sets the wavespeed at the
+            # outer boundary
+            self.aux = None
+            return
         self.aux = np.zeros(abi.NUM_AUXEVOL_GFS * self.Ntot)
         lib.nrpyell_auxevol_gfs_all_points(C.byref(p), self.xx, _ptr(self.aux))
         lib.nrpyell_wavespeed_gf_all_points(C.byref(p), cfg.CFL, self.dt, self.xx, _ptr(self.aux))
-        c = lib.nrpyell_compute_wavespeed_at_OB(C.byref(p), _ptr(self.aux))
-        p.uu_wavespeed_at_OB = c
-        p.vv_wavespeed_at_OB = c
-        self._closed = False
+        self.set_wavespeed_at_OB(lib.nrpyell_compute_wavespeed_at_OB(C.byref(p), _ptr(self.aux)))
+
+    def set_wavespeed_at_OB(self, c):
+        self.params.uu_wavespeed_at_OB = c
+        self.params.vv_wavespeed_at_OB = c
+
+    def wavespeed_OB_index(self):
+        """Index in the wavespeed gridfunction read by compute_wavespeed_at_OB.c:10."""
+        N0, N1, N2 = self.N
+        return (N0 - abi.NGHOSTS - 1) + N0 * (abi.NGHOSTS + N1 * (N2 // 2))
 
     # numpy views
     def xx_arrays(self):
@@ -196,7 +209,7 @@ class Problem:
 class DeviceState:
     """Device buffers of one problem (y_n, running total, k_odd, k_even,
     auxevol) allocated through the library; the auxevol gridfunctions are
-    uploaded once."""
+    uploaded once, or computed on the GPU when the problem has no host copy."""
 
     def __init__(self, prob, lib=None):
         self.lib = lib = lib or prob.lib
@@ -205,7 +218,15 @@ class DeviceState:
         self.ptr = {k: lib.nrpyell_device_malloc(n2) for k in ("y_n", "acc", "k_odd", "k_even")}
         self.ptr["aux"] = lib.nrpyell_device_malloc(abi.NUM_AUXEVOL_GFS * prob.Ntot * 8)
         _lib.check(lib)
-        self.upload("aux", prob.aux)
+        if prob.aux is not None:
+            self.upload("aux", prob.aux)
+        else:
+            lib.nrpyell_auxevol_device(C.byref(prob.params), prob.xx, prob.cfg.CFL, prob.dt, self.dptr("aux"))
+            _lib.check(lib)
+            ws = np.zeros(1)
+            off = (abi.WAVESPEEDGF * prob.Ntot + prob.wavespeed_OB_index()) * 8
+            lib.nrpyell_memcpy(ws.ctypes.data, self.ptr["aux"] + off, 8, 1)
+            prob.set_wavespeed_at_OB(float(ws[0]))
         self.set_state(prob.zero_state())
         for k in ("acc", "k_odd", "k_even"):
             lib.nrpyell_memset(self.ptr[k], 0, n2)

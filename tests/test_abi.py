@@ -67,3 +67,21 @@ def test_status_api_without_gpu_work():
     assert lib.nrpyell_get_step_mode() == 1
     lib.nrpyell_set_step_mode(0)
     assert lib.nrpyell_get_step_mode() == 0
+
+
+def test_optimum_eta_damping_formula():
+    """Eq. (B6) and (36) of arXiv:2111.02424 as the thorn evaluates them."""
+    import math
+
+    import pytest
+
+    from nrpyelliptic_b200.problem import CONFIGS, Problem
+    lib = _lib.load()
+    prob = Problem(CONFIGS["quasicircular_128x128x16"], lib=lib)
+    p = prob.params
+    A, b, dt = p.AMAX, p.bScale, prob.dt
+    c1 = math.cos(p.dxx1 / 2)
+    trc = dt / (0.5 * p.dxx1) * math.atanh(A / math.sqrt(A * A + b * b * c1 * c1)) * c1 * math.cos(p.dxx2 / 2)
+    assert lib.nrpyell_compute_TRC(A, b, 0.5, dt, p.dxx1, p.dxx2) == pytest.approx(trc, rel=1e-14)
+    lib.nrpyell_set_optimum_eta_damping(dt, 0.5, C.byref(p))
+    assert p.eta_damping == pytest.approx(6.9 * trc ** -0.79 - 0.7, rel=1e-14)

@@ -64,3 +64,20 @@ def test_batch_autotuned_tile_converges(lib):
     assert rc == 0 and np.all(finals <= -10.0) and np.all(steps > 0)
     for s in states:
         s.free()
+
+
+def test_auxevol_on_the_gpu_matches_the_host_set_up(lib):
+    """nrpyell_auxevol_device against the host restatement, each gridfunction
+    within 1e-13 of its largest value (same closed forms, compiled for the
+    device and for the host)."""
+    from nrpyelliptic_b200 import abi
+    for cfg in (CONFIGS["shipped_64x64x8"], with_grid(sample_sweep(3)[2], (48, 40, 8))):
+        host = Problem(cfg, lib=lib)
+        dev = Problem(cfg, lib=lib, host_aux=False)
+        ds = DeviceState(dev, lib=lib)
+        aux = ds.download("aux").reshape(abi.NUM_AUXEVOL_GFS, -1)
+        ref = host.aux.reshape(abi.NUM_AUXEVOL_GFS, -1)
+        for g in range(abi.NUM_AUXEVOL_GFS):
+            assert np.max(np.abs(aux[g] - ref[g])) <= 1e-13 * np.max(np.abs(ref[g])), (cfg.name, g)
+        assert dev.params.uu_wavespeed_at_OB == pytest.approx(host.params.uu_wavespeed_at_OB, rel=1e-14)
+        ds.free()

@@ -277,3 +277,33 @@ def test_unmodified_main_c_links_and_matches_reference(tmp_path):
     uu_cpu = np.loadtxt(a / "output_NRPyElliptic" / "uu_final_1D.txt")
     uu_gpu = np.loadtxt(b / "output_NRPyElliptic" / "uu_final_1D.txt")
     assert np.max(np.abs(uu_gpu[:, 1] - uu_cpu[:, 1])) <= 1e-12 * np.max(np.abs(uu_cpu[:, 1]))
+
+
+def test_python_playground_writes_main_c_files(tmp_path):
+    """python -m nrpyelliptic_b200.playground with --snapshots writes the same
+    files as the reference executable, with the same coordinates and values
+    within the parity tolerances."""
+    ref_exe = os.path.join(ROOT, "oracle", "_ref", "NRPyElliptic_Playground")
+    if not os.path.exists(ref_exe):
+        pytest.skip("the reference executable is built only where the reference sources exist")
+    a = tmp_path / "cpu"
+    b = tmp_path / "gpu"
+    a.mkdir()
+    b.mkdir()
+    args = ["32", "16", "8", "120"]
+    _run_playground(ref_exe, str(a), args)
+    from nrpyelliptic_b200 import playground
+    assert playground.main(args + ["--snapshots", "--outdir", str(b)]) == 0
+    ra, rb = a / "output_NRPyElliptic", b / "output_NRPyElliptic"
+    names = sorted(str(p.relative_to(ra)) for p in ra.rglob("*") if p.is_file())
+    assert names == sorted(str(p.relative_to(rb)) for p in rb.rglob("*") if p.is_file())
+    for name in names:
+        x, y = np.loadtxt(ra / name, ndmin=2), np.loadtxt(rb / name, ndmin=2)
+        assert x.shape == y.shape, name
+        if name == "residual_l2_norm.txt":
+            np.testing.assert_array_equal(x[:, :2], y[:, :2])
+            np.testing.assert_allclose(y[:, 2], x[:, 2], rtol=0, atol=1e-10)
+            continue
+        np.testing.assert_allclose(y[:, :-1], x[:, :-1], rtol=1e-14, atol=1e-12, err_msg=name)
+        scale = max(np.max(np.abs(x[:, -1])), 1e-300)
+        assert np.max(np.abs(y[:, -1] - x[:, -1])) <= 1e-10 * scale, name
