@@ -113,6 +113,7 @@ def main(argv=None):
     hist = []
     n, rc, fin = 0, 1, C.c_double(0.0)
     while True:
+        # main.c:145-179: the residual and the snapshots of step n, then the step
         if a.snapshots and not a.no_output and n % every == 0:
             write_rows(os.path.join(out, "1D", "uu_1D_%08d.dat" % n), z_axis_dump(prob, ds.download("y_n")[:prob.Ntot]),
                        "%.17e %.17e\n")
@@ -123,6 +124,8 @@ def main(argv=None):
             _lib.check(lib)
             write_rows(os.path.join(out, "2D", "residual_2D_%08d.dat" % n),
                        xz_plane_dump(prob, ds.download("acc")[:prob.Ntot]), "%.17e %.17e %.17e\n")
+        if hist and (rc == 0 or n >= a.N_final):
+            break
         chunk = min(every, a.N_final - n)
         h = np.zeros(chunk + 1)
         steps = C.c_int(0)
@@ -131,7 +134,7 @@ def main(argv=None):
         _lib.check(lib)
         hist.extend(h[(1 if hist else 0):steps.value + 1])
         n += steps.value
-        if rc == 0 or n >= a.N_final or steps.value < chunk:
+        if steps.value < chunk and rc != 0:
             break
     if a.tol is None:
         # main.c's loop also steps after its last residual (n = N_final)
