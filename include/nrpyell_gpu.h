@@ -132,7 +132,9 @@ void nrpyell_set_async(int enable);
  * same with the pointwise inputs loaded before the first store; 3 TMA
  * pipeline (persistent CTAs, tiles staged by tensor-map bulk copies, FP64
  * only -- FP32 runs shape kind 2 instead); 4 the block's uu planes staged in
- * shared memory. */
+ * shared memory; 5 the block marches through `planes` i2 planes, each plane
+ * and its pointwise inputs copied into shared memory ahead of use by
+ * asynchronous copies. */
 void nrpyell_set_tile(int tile);
 int nrpyell_get_tile(const paramstruct *params, int fp32, int *bx, int *by, int *planes);
 int nrpyell_num_tiles(void);

@@ -76,6 +76,13 @@ void launch_columns_forked(int stage, const SubstepArgs& a);
 void join_columns();
 void prepare_columns();
 
+// ---- marching variant (kernels_march.cu): shape v of the list there
+template <typename T>
+void launch_march(int stage, bool resid, int v, const SubstepArgs& a);
+// Shared-memory opt-in of a shape's kernels (before a stream capture).
+template <typename T>
+void prepare_march(int v);
+
 // ---- bulk-copy pipeline variant (kernels_bulk.cu), FP64 ----
 // Usable when the row length N0 is even and every array is 16-byte aligned.
 bool bulk_available(const SubstepArgs& a, size_t elem_size);

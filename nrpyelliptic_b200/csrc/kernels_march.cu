@@ -1,0 +1,286 @@
+// Fused RK4 substep, marching variant (tile kind 5).
+//
+// Same substep and the same per-point arithmetic as the planes kernel of
+// kernels_fused.cu, so every step is bit-identical to it; what differs is how
+// uu reaches the stencil.  An interior block owns a 32 x BY tile of (i0,i1)
+// columns and PZ consecutive i2 planes, and walks its planes in order:
+//   * each plane of uu, widened by 5 points along i0 and i1, and the plane's
+//     pointwise inputs (vv of the stage input, the three auxevol fields, y_n
+//     and the running total) are copied into shared memory by asynchronous
+//     copies (cp.async), issued D-1 planes ahead into a ring of D slots, so
+//     the loads of the next D-1 planes are in flight while plane p is
+//     computed and the block needs one barrier per plane;
+//   * uu along i2 at the thread's own column is a register queue (the 10
+//     planes around the first one loaded up front, then one value per plane
+//     delivered with the slot), so the i2 stencil arm costs no extra load;
+//   * the six metric weights of the column (and the L2 weight) are loaded
+//     once per block.
+// Per interior point this reads uu from L2 about 2.9-4.6 times (plane halo)
+// plus (PZ+10)/PZ times (queue), against 14-16 times in the one-plane planes
+// kernel, and the pointwise inputs arrive without a register cost.
+// Column blocks (the radiation BC of the x0max face) come first in the
+// launch, as in the planes kernel.
+#include "substep.cuh"
+
+namespace nrpyell {
+
+namespace {
+
+__device__ __forceinline__ unsigned smem_u32(const void* p) { return (unsigned)__cvta_generic_to_shared(p); }
+
+// Asynchronous global -> shared copy of BYTES (4, 8: through L1; 16: L2 only).
+template <int BYTES>
+__device__ __forceinline__ void cp_async(void* dst, const void* src) {
+  if (BYTES == 16)
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(smem_u32(dst)), "l"(src) : "memory");
+  else
+    asm volatile("cp.async.ca.shared.global [%0], [%1], %2;\n" ::"r"(smem_u32(dst)), "l"(src), "n"(BYTES)
+                 : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
+template <int N>
+__device__ __forceinline__ void cp_async_wait() {
+  asm volatile("cp.async.wait_group %0;\n" ::"n"(N) : "memory");
+}
+
+// Shared memory of one block, in elements of T per ring slot: the widened uu
+// plane [BY+10][42], then NPF pointwise rows of NT values (vv, ADD_TIMES_AUU,
+// psi_background, wavespeed, y_n uu, y_n vv, uu at i2+5, and from stage 2 on
+// the running totals of uu and vv).  Rows of 42 doubles are 336 bytes, so
+// every row starts on a 16-byte boundary.  (The pointwise fields are copied
+// per point: 16-byte pieces of their rows, from i0 = i00-1, were slower.)
+template <typename T, int BY, int STAGE, int D>
+struct MarchSmem {
+  static constexpr int NT = 32 * BY, NR = BY + 10, RWS = 42;
+  static constexpr int NPF = STAGE == 1 ? 7 : 9;
+  static constexpr int plane = NR * RWS;
+  static constexpr int slot = plane + NPF * NT;
+  static constexpr size_t march = (size_t)D * slot * sizeof(T);
+  static constexpr size_t bytes = march > sizeof(double) * kRowsSmem ? march : sizeof(double) * kRowsSmem;
+};
+
+template <typename T, int STAGE, bool RESID, int BY, int PZ, int D, int MINB>
+__global__ void __launch_bounds__(32 * BY, MINB) k_substep_march(SubDev<T> a) {
+  extern __shared__ __align__(16) double dsm[];
+  __shared__ double sh[BY > 8 ? BY : 8];
+  __shared__ bool last;
+  if (*a.done) return;
+  using L = MarchSmem<T, BY, STAGE, D>;
+  constexpr int NT = L::NT, NR = L::NR, RWS = L::RWS, HALF = RWS / 2;
+  const int bid = blockIdx.x;
+  if (bid < a.n_col_blocks) {
+    column_rows<T, STAGE, NT>(a, bid, dsm);
+    return;
+  }
+  T* const ring = reinterpret_cast<T*>(dsm);
+  const int tid = threadIdx.x, tx = tid & 31, ty = tid >> 5;
+  const int b = bid - a.n_col_blocks;
+  const int t0 = b % a.tiles0, t1 = (b / a.tiles0) % a.tiles1, t2 = b / (a.tiles0 * a.tiles1);
+  const int i00 = t0 * 32 + NGHOSTS, i10 = t1 * BY + NGHOSTS, z0 = t2 * PZ + NGHOSTS;
+  const int N0 = a.N0, top = NGHOSTS + a.Nxx1;
+  const int nz = min(PZ, NGHOSTS + a.Nxx2 - z0);
+  const long long N01 = a.N01, Ntot = a.Ntot;
+  const T* __restrict__ u = a.S;
+  // tiles whose widened planes reach an inner ghost zone gather each point
+  // from its source; the others copy rows (16-byte pieces for FP64 when the
+  // rows are 16-byte aligned: N0 even and an aligned array)
+  const bool inner = (t0 == 0) || (i10 < 2 * NGHOSTS) || (i10 + BY + NGHOSTS > top);
+  const bool vec = sizeof(T) == 8 && !inner && (N0 & 1) == 0 && (reinterpret_cast<size_t>(u) & 15) == 0;
+  const int i0 = i00 + tx, i1 = i10 + ty;
+  const bool valid = i0 < NGHOSTS + a.Nxx0 && i1 < top;
+  const int k2 = i0 + N0 * i1;
+
+  // copies of plane p into ring slot p % D (one commit group per plane, empty
+  // past the block's last plane)
+  auto issue = [&](int p) {
+    if (p < nz) {
+      T* su = ring + (p % D) * L::slot;
+      T* pf = su + L::plane;
+      const int i2 = z0 + p;
+      if (vec) {
+        const T* src = u + (i00 - NGHOSTS) + (long long)N0 * (i10 - NGHOSTS) + N01 * i2;
+        for (int e = tid; e < NR * HALF; e += NT) {
+          const int r = e / HALF, c = 2 * (e - r * HALF);
+          if (i00 - NGHOSTS + c < N0) cp_async<16>(su + r * RWS + c, src + (long long)N0 * r + c);
+        }
+      } else {
+        for (int e = tid; e < NR * RWS; e += NT) {
+          const int r = e / RWS, x = e - r * RWS;
+          int j0 = i00 - NGHOSTS + x, j1 = i10 - NGHOSTS + r, j2 = i2;
+          if (j0 >= N0 || j1 >= top + NGHOSTS) continue;  // never read
+          if (inner) {
+            bool flip = false;
+            if (j1 < NGHOSTS) {
+              j1 = 2 * NGHOSTS - 1 - j1;
+              flip = true;
+            } else if (j1 >= top) {
+              j1 = 2 * top - 1 - j1;
+              flip = true;
+            }
+            if (j0 < NGHOSTS) {
+              j0 = 2 * NGHOSTS - 1 - j0;
+              flip = !flip;
+            }
+            if (flip) j2 = wrap2(i2 + a.half2, a.Nxx2);
+          }
+          cp_async<(int)sizeof(T)>(su + r * RWS + x, u + j0 + (long long)N0 * j1 + N01 * j2);
+        }
+      }
+      if (valid) {
+        const long long idx = k2 + N01 * i2;
+        cp_async<(int)sizeof(T)>(pf + 0 * NT + tid, a.S + Ntot + idx);
+        cp_async<(int)sizeof(T)>(pf + 1 * NT + tid, a.aux + ADD_TIMES_AUUGF * Ntot + idx);
+        cp_async<(int)sizeof(T)>(pf + 2 * NT + tid, a.aux + PSI_BACKGROUNDGF * Ntot + idx);
+        cp_async<(int)sizeof(T)>(pf + 3 * NT + tid, a.aux + WAVESPEEDGF * Ntot + idx);
+        cp_async<(int)sizeof(T)>(pf + 4 * NT + tid, a.y + idx);
+        cp_async<(int)sizeof(T)>(pf + 5 * NT + tid, a.y + Ntot + idx);
+        cp_async<(int)sizeof(T)>(pf + 6 * NT + tid, u + k2 + N01 * wrapm(i2 + NGHOSTS, a.Nxx2));
+        if (STAGE != 1) {
+          cp_async<(int)sizeof(T)>(pf + 7 * NT + tid, a.acc + idx);
+          cp_async<(int)sizeof(T)>(pf + 8 * NT + tid, a.acc + Ntot + idx);
+        }
+      }
+    }
+    cp_async_commit();
+  };
+
+#pragma unroll
+  for (int p = 0; p < D - 1; p++) issue(p);
+  // uu along i2: q[j] is plane z0-5+j
+  T q[PZ + 10];
+  T C22 = 0, C00 = 0, C11 = 0, C1 = 0, C0 = 0, Cc = 0;
+  double wl2 = 0.0;
+  if (valid) {
+#pragma unroll
+    for (int j = 0; j < 10; j++) q[j] = __ldg(u + k2 + N01 * wrapm(z0 - NGHOSTS + j, a.Nxx2));
+    C22 = __ldg(a.coef + k2);
+    C00 = __ldg(a.coef + N01 + k2);
+    C11 = __ldg(a.coef + 2 * N01 + k2);
+    C1 = __ldg(a.coef + 3 * N01 + k2);
+    C0 = __ldg(a.coef + 4 * N01 + k2);
+    Cc = __ldg(a.coef + 5 * N01 + k2);
+    if (RESID) wl2 = __ldg(a.w + k2);
+  }
+  double r2 = 0.0;
+#pragma unroll
+  for (int p = 0; p < PZ; p++) {
+    if (p >= nz) break;      // uniform over the block
+    cp_async_wait<D - 2>();  // this thread's copies of plane p have landed
+    __syncthreads();         // everyone's have; slot (p+D-1)%D was last read at plane p-1
+    issue(p + D - 1);
+    if (valid) {
+      const T* su = ring + (p % D) * L::slot;
+      const T* pf = su + L::plane + tid;  // this point's pointwise fields, stride NT
+      q[p + 10] = pf[6 * NT];
+      const T* sp = su + (ty + NGHOSTS) * RWS + tx + NGHOSTS;
+      T s0 = 0, s1 = 0, s00 = 0, s11 = 0, s22 = 0;
+#pragma unroll
+      for (int k = 1; k <= 5; k++) {
+        const T am = sp[-k], ap = sp[k];
+        const T bm = sp[-k * RWS], bp = sp[k * RWS];
+        s0 = fma(W<T>::d(k), ap - am, s0);
+        s1 = fma(W<T>::d(k), bp - bm, s1);
+        s00 = fma(W<T>::e(k), ap + am, s00);
+        s11 = fma(W<T>::e(k), bp + bm, s11);
+      }
+#pragma unroll
+      for (int k = 1; k <= 5; k++) s22 = fma(W<T>::e(k), q[p + 5 + k] + q[p + 5 - k], s22);
+      T ku, kv, br;
+      constexpr int FS = NT;
+      point_rhs<T>(q[p + 5], pf[0], pf[FS], pf[2 * FS], pf[3 * FS], C22, C00, C11, C1, C0, Cc, s0, s1, s00, s11, s22,
+                   a.eta, ku, kv, br);
+      const T accu = (STAGE == 1) ? (T)0 : pf[7 * FS];
+      const T accv = (STAGE == 1) ? (T)0 : pf[8 * FS];
+      store_point<T, STAGE>(a, k2 + N01 * (z0 + p), ku, kv, pf[4 * FS], pf[5 * FS], accu, accv);
+      if (RESID) {
+        const double bb = (double)br;
+        r2 += bb * bb * wl2;
+      }
+    }
+  }
+  if (RESID && tile_partial<NT>(r2, b, a.partials, a.ticket, a.n_tiles, sh, &last)) finalize_l2<T, NT>(a, sh);
+}
+
+// Opts the kernel into more than 48 KB of dynamic shared memory, once per
+// device.
+template <typename T, int STAGE, bool RESID, int BY, int PZ, int D, int MINB>
+bool march_opt_in() {
+  static unsigned long long devices = 0;
+  const size_t bytes = MarchSmem<T, BY, STAGE, D>::bytes;
+  if (bytes <= 48 * 1024) return true;
+  int dev = 0;
+  NRPYELL_CUDA(cudaGetDevice(&dev));
+  if (dev >= 0 && dev < 64 && !(devices >> dev & 1ull)) {
+    NRPYELL_CUDA(cudaFuncSetAttribute(k_substep_march<T, STAGE, RESID, BY, PZ, D, MINB>,
+                                      cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes));
+    devices |= 1ull << dev;
+  }
+  return status_ok();
+}
+
+template <typename T, int STAGE, bool RESID, int BY, int PZ, int D, int MINB>
+void launch_march_shape(const SubstepArgs& a) {
+  if (!march_opt_in<T, STAGE, RESID, BY, PZ, D, MINB>()) return;
+  SubDev<T> f = make_dev<T>(a, BY, PZ);
+  f.n_col_blocks = ((a.d.Nxx1 + kRows - 1) / kRows) * a.d.Nxx2;
+  NRPYELL_LAUNCH((k_substep_march<T, STAGE, RESID, BY, PZ, D, MINB>), f.n_tiles + f.n_col_blocks, 32 * BY,
+                 (MarchSmem<T, BY, STAGE, D>::bytes), f);
+}
+
+// The compiled shapes, by index: (BY, PZ, ring slots D, minimum resident
+// blocks per SM for the register budget).
+#define NRPYELL_MARCH_SHAPES(X)                                                                           \
+  X(0, 8, 8, 3, 2) X(1, 8, 8, 2, 4) X(2, 8, 4, 2, 4) X(3, 8, 16, 2, 4) X(4, 4, 8, 2, 8) X(5, 4, 4, 2, 8) \
+      X(6, 8, 4, 3, 2)
+
+template <typename T, int STAGE, bool RESID>
+bool march_stage(int v, const SubstepArgs& a) {
+  switch (v) {
+#define NRPYELL_MARCH(I, BY, PZ, D, MINB)                          \
+  case I:                                                          \
+    launch_march_shape<T, STAGE, RESID, BY, PZ, D, MINB>(a);       \
+    return true;
+    NRPYELL_MARCH_SHAPES(NRPYELL_MARCH)
+#undef NRPYELL_MARCH
+  }
+  return false;
+}
+
+template <typename T, int BY, int PZ, int D, int MINB>
+void opt_in_shape() {
+  march_opt_in<T, 1, true, BY, PZ, D, MINB>();
+  march_opt_in<T, 1, false, BY, PZ, D, MINB>();
+  march_opt_in<T, 2, false, BY, PZ, D, MINB>();
+  march_opt_in<T, 3, false, BY, PZ, D, MINB>();
+  march_opt_in<T, 4, false, BY, PZ, D, MINB>();
+}
+
+}  // namespace
+
+template <typename T>
+void launch_march(int stage, bool resid, int v, const SubstepArgs& a) {
+  bool ok = false;
+  switch (stage) {
+    case 1: ok = resid ? march_stage<T, 1, true>(v, a) : march_stage<T, 1, false>(v, a); break;
+    case 2: ok = march_stage<T, 2, false>(v, a); break;
+    case 3: ok = march_stage<T, 3, false>(v, a); break;
+    default: ok = march_stage<T, 4, false>(v, a); break;
+  }
+  if (!ok) NRPYELL_FAIL("launch_march: no kernel for this shape");
+}
+template void launch_march<double>(int, bool, int, const SubstepArgs&);
+template void launch_march<float>(int, bool, int, const SubstepArgs&);
+
+template <typename T>
+void prepare_march(int v) {
+  switch (v) {
+#define NRPYELL_MARCH(I, BY, PZ, D, MINB) \
+  case I: opt_in_shape<T, BY, PZ, D, MINB>(); break;
+    NRPYELL_MARCH_SHAPES(NRPYELL_MARCH)
+#undef NRPYELL_MARCH
+  }
+}
+template void prepare_march<double>(int);
+template void prepare_march<float>(int);
+
+}  // namespace nrpyell

@@ -371,6 +371,116 @@ __device__ void column_block(const SubDev<T>& a, int cb) {
   }
 }
 
+// ------------------------------------------------ radiation columns by rows
+// The radiation BC of the x0max face: the column blocks of the shared-memory
+// planes kernel, and a kernel of its own that runs beside the persistent TMA
+// pipeline kernel on the side stream.  A block takes
+// kRows consecutive i1 columns at one i2: it copies the outer 12 points of
+// uu and vv along i0 on those rows and on 5 rows either side (rows across
+// the axis from their images) into shared memory, then computes every
+// column's 12 radial derivatives, the RHS of its last interior point, the
+// layer recurrence and the RK combination with the same arithmetic as
+// column_block.
+constexpr int kRows = 32;
+
+// Shared memory of column_rows, in doubles: F[2][kRows+10][12], drf and fvs
+// [kRows][2][6], kl [kRows][2], kk [kRows][2][5].
+constexpr int kRowsSmem = 2 * (kRows + 10) * 12 + 2 * kRows * 12 + kRows * 2 + kRows * 10;
+
+template <typename T, int STAGE, int NT>
+__device__ void column_rows(const SubDev<T>& a, int cb, double* smem) {
+  static_assert(NT >= 2 * kRows, "the layer recurrence takes one thread per column and gridfunction");
+  constexpr int NRW = kRows + 10, NQ = 12;
+  double(*F)[NRW][NQ] = reinterpret_cast<double(*)[NRW][NQ]>(smem);
+  double(*drf)[2][6] = reinterpret_cast<double(*)[2][6]>(smem + 2 * NRW * NQ);
+  double(*fvs)[2][6] = reinterpret_cast<double(*)[2][6]>(smem + 2 * NRW * NQ + kRows * 12);
+  double(*kl)[2] = reinterpret_cast<double(*)[2]>(smem + 2 * NRW * NQ + 2 * kRows * 12);
+  double(*kk)[2][5] = reinterpret_cast<double(*)[2][5]>(smem + 2 * NRW * NQ + 2 * kRows * 12 + 2 * kRows);
+  const int tid = threadIdx.x;
+  const int nb1 = (a.Nxx1 + kRows - 1) / kRows;
+  const int i1a = NGHOSTS + (cb % nb1) * kRows;
+  const int i2 = NGHOSTS + cb / nb1;
+  const int top = NGHOSTS + a.Nxx1;
+  const int ncol = min(kRows, top - i1a);
+  const int i2h = wrap2(i2 + a.half2, a.Nxx2);
+  const int N0 = a.N0;
+  for (int e = tid; e < 2 * NRW * NQ; e += NT) {
+    const int q = e % NQ, j = (e / NQ) % NRW, g = e / (NQ * NRW);
+    if (j >= ncol + 2 * NGHOSTS) continue;  // not needed
+    int i1 = i1a - NGHOSTS + j, i2s = i2;
+    if (i1 < NGHOSTS) {
+      i1 = 2 * NGHOSTS - 1 - i1;
+      i2s = i2h;
+    } else if (i1 >= top) {
+      i1 = 2 * top - 1 - i1;
+      i2s = i2h;
+    }
+    F[g][j][q] = (double)__ldg(a.S + g * a.Ntot + (N0 - NQ + q) + (long long)N0 * i1 + a.N01 * i2s);
+  }
+  __syncthreads();
+  // radial derivatives at the last interior point and the 5 layers (items
+  // c*12 + g*6 + jj), then the RHS of each column's last interior point
+  for (int it = tid; it < kRows * 13; it += NT) {
+    if (it < kRows * 12) {
+      const int c = it / 12, g = (it / 6) % 2, jj = it % 6;
+      if (c >= ncol) continue;
+      const int off = (jj <= 1) ? -1 : -jj;
+      double v[11];
+#pragma unroll
+      for (int m = 0; m < 11; m++) v[m] = F[g][c + NGHOSTS][1 + jj + off + m];
+      const double d0 = radiation_sum_x0(c_fd1w[off + 5], v);
+#pragma unroll
+      for (int m = 0; m < 11; m++) v[m] = (m == 5) ? 0.0 : F[g][c + m][6 + jj];
+      const double d1 = radiation_sum_x1(v);
+      const int i1 = i1a + c;
+      drf[c][g][jj] = radiation_drf(d0, d1, a.invdx0, a.invdx1, __ldg(a.colgeo + (1 * 6 + jj) * a.N1 + i1),
+                                    __ldg(a.colgeo + (2 * 6 + jj) * a.N1 + i1));
+      fvs[c][g][jj] = F[g][c + NGHOSTS][6 + jj];
+    } else {
+      const int c = it - kRows * 12;
+      if (c >= ncol) continue;
+      const int i1 = i1a + c, i0 = N0 - NGHOSTS - 1;
+      const double* row = F[0][c + NGHOSTS];
+      T s0 = 0, s1 = 0, s00 = 0, s11 = 0, s22 = 0;
+#pragma unroll
+      for (int k = 1; k <= 5; k++) {
+        const T am = (T)row[6 - k], ap = (T)row[6 + k];
+        const T bm = (T)F[0][c + NGHOSTS - k][6], bp = (T)F[0][c + NGHOSTS + k][6];
+        s0 = fma(W<T>::d(k), ap - am, s0);
+        s1 = fma(W<T>::d(k), bp - bm, s1);
+        s00 = fma(W<T>::e(k), ap + am, s00);
+        s11 = fma(W<T>::e(k), bp + bm, s11);
+      }
+      const T* u = a.S;
+      const long long line = i0 + (long long)N0 * i1;
+#pragma unroll
+      for (int k = 1; k <= 5; k++)
+        s22 = fma(W<T>::e(k),
+                  __ldg(u + line + a.N01 * wrap2(i2 + k, a.Nxx2)) + __ldg(u + line + a.N01 * wrap2(i2 - k, a.Nxx2)),
+                  s22);
+      T ku, kv, br;
+      point_rhs_global<T>(a, line + a.N01 * i2, i0 + N0 * i1, (T)row[6], s0, s1, s00, s11, s22, ku, kv, br);
+      kl[c][0] = (double)ku;
+      kl[c][1] = (double)kv;
+    }
+  }
+  __syncthreads();
+  if (tid < 2 * ncol) {
+    const int c = tid / 2, g = tid % 2;
+    radiation_layers((double)a.cOB[g], kl[c][g], drf[c][g], fvs[c][g], a.colgeo + i1a + c, a.N1, kk[c][g]);
+  }
+  __syncthreads();
+  for (int it = tid; it < ncol * 10; it += NT) {
+    const int c = it / 10, g = (it / 5) % 2, L = it % 5;
+    const long long idx = g * a.Ntot + (long long)N0 * (i1a + c) + a.N01 * i2 + N0 - NGHOSTS + L;
+    T accv = (STAGE == 1) ? (T)0 : a.acc[idx];
+    T ov;
+    rk_combine<T, STAGE>((T)kk[c][g][L], a.y[idx], accv, ov, a.dt);
+    if (STAGE != 4) a.acc[idx] = accv;
+    a.out[idx] = ov;
+  }
+}
+
 // Interior index along i2 for any j (a tile that runs past the last plane
 // can reach more than one wrap on short grids).
 __device__ __forceinline__ int wrapm(int j, int Nxx2) {

@@ -42,7 +42,7 @@ def tiles(lib):
 
 def test_tile_table_has_every_kind(lib):
     tl = tiles(lib)
-    assert {k for *_, k in tl} == {0, 2, 3, 4}
+    assert {k for *_, k in tl} == {0, 2, 3, 4, 5}
     assert lib.nrpyell_tile_info(len(tl), None, None, None) == -1
 
 
@@ -106,7 +106,7 @@ def test_shared_memory_tiles_in_mixed_precision(lib):
     ref = gold["uu_interior"]
     try:
         for t, by, p, kind in tiles(lib):
-            if kind not in (3, 4):
+            if kind not in (3, 4, 5):
                 continue
             lib.nrpyell_set_tile(t)
             ds = DeviceState(prob)
