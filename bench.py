@@ -102,15 +102,19 @@ def measured_hbm_peak():
         return 6650.0, "fallback"
 
 
-def profiled_traffic(tag):
-    """DRAM bytes per launch of the fused interior kernel recorded from ncu in
-    profiles/ (a line 'dram_bytes_per_launch[<tag>]: <n>'), else None."""
+# Fused substep kernel of each tile kind (nrpyell_tile_info).
+KERNELS = {0: "k_substep", 2: "k_substep", 3: "k_substep_bulk", 4: "k_substep_planes", 5: "k_substep_march"}
+
+
+def profiled_traffic(kernel, tag):
+    """DRAM bytes per launch of a fused substep kernel recorded from ncu in
+    profiles/ (a line 'dram_bytes_per_launch[<kernel> <tag>]: <n>'), else None."""
     try:
         for name in os.listdir(os.path.join(ROOT, "profiles")):
             if not name.endswith((".md", ".txt")):
                 continue
             for line in open(os.path.join(ROOT, "profiles", name)):
-                key = "dram_bytes_per_launch[%s]:" % tag
+                key = "dram_bytes_per_launch[%s %s]:" % (kernel, tag)
                 if key in line:
                     return float(line.split(key)[1].split()[0])
     except Exception:
@@ -323,13 +327,20 @@ def run_ours(args, dist):
     lib.nrpyell_time_fused(C.byref(ds.g), prob.dt, 2, 200, C.byref(ms_k), C.byref(ms_s))
     _lib.check(lib)
     bx, by, planes = C.c_int(0), C.c_int(0), C.c_int(0)
-    lib.nrpyell_get_tile(C.byref(prob.params), 0, C.byref(bx), C.byref(by), C.byref(planes))
+
+    def kernel_of(tile):
+        kind = C.c_int(-1)
+        lib.nrpyell_tile_info(tile, None, None, C.byref(kind))
+        return KERNELS.get(kind.value, "k_substep")
+
+    t_small = lib.nrpyell_get_tile(C.byref(prob.params), 0, C.byref(bx), C.byref(by), C.byref(planes))
     tile = [bx.value, by.value, planes.value]
+    kern = kernel_of(t_small)
     achieved = ALG_BYTES_STAGE2 * n_int / (ms_k.value * 1e-3) / 1e9
     tag = "%dx%dx%d" % cfg.Nxx
-    traffic = profiled_traffic(tag)
+    traffic = profiled_traffic(kern, tag)
     roofline = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
-                "traffic": traffic, "kernel": "k_substep<double,2>", "tile": tile, "peak_kind": peak_kind,
+                "traffic": traffic, "kernel": "%s<double,2>" % kern, "tile_index": t_small, "tile": tile, "peak_kind": peak_kind,
                 "alg_bytes_per_launch": ALG_BYTES_STAGE2 * n_int, "us_per_launch": ms_k.value * 1e3,
                 "rk4_step_us": ms_s.value * 1e3,
                 "rk4_step_GBps": ALG_BYTES_STEP * n_int / (ms_s.value * 1e-3) / 1e9,
@@ -339,12 +350,13 @@ def run_ours(args, dist):
     dsb = DeviceState(big)
     lib.nrpyell_time_fused(C.byref(dsb.g), big.dt, 2, 50, C.byref(ms_k), C.byref(ms_s))
     _lib.check(lib)
-    lib.nrpyell_get_tile(C.byref(big.params), 0, C.byref(bx), C.byref(by), C.byref(planes))
+    t_big = lib.nrpyell_get_tile(C.byref(big.params), 0, C.byref(bx), C.byref(by), C.byref(planes))
+    kern_b = kernel_of(t_big)
     nb = 256 * 256 * 32
     ach_b = ALG_BYTES_STAGE2 * nb / (ms_k.value * 1e-3) / 1e9
     roofline_big = {"bound": "hbm", "achieved": ach_b, "peak": peak, "unit": "GB/s", "frac": ach_b / peak,
-                    "traffic": profiled_traffic("256x256x32"), "kernel": "k_substep<double,2>",
-                    "tile": [bx.value, by.value, planes.value],
+                    "traffic": profiled_traffic(kern_b, "256x256x32"), "kernel": "%s<double,2>" % kern_b,
+                    "tile_index": t_big, "tile": [bx.value, by.value, planes.value],
                     "grid": "256x256x32", "us_per_launch": ms_k.value * 1e3, "rk4_step_us": ms_s.value * 1e3,
                     "rk4_step_GBps": ALG_BYTES_STEP * nb / (ms_s.value * 1e-3) / 1e9}
     dsb.free()
