@@ -105,6 +105,7 @@ SubstepArgs substep_args(const Dims& d, RfmTables* rt, BcTables* bt, Scratch* s,
   a.log10_tol = -1e300;
   a.max_steps = 0;
   a.check_every = 0;
+  a.defer_l2 = 0;
   a.stall = nullptr;
   a.stall_window = 0;
   a.stall_log_drop = 0.0;
@@ -211,6 +212,7 @@ RelaxResult relax_loop(const Dims& d, RfmTables* rt, BcTables* bt, L2Tables* lt,
     cudaGraph_t graph;
     const long long launches_before = launch_count();
     prepare_substep<T>(tile);
+    prepare_columns();
     NRPYELL_CUDA(cudaStreamBeginCapture(stream(), cudaStreamCaptureModeThreadLocal));
     for (int k = 0; k < kStepsPerGraph; k++) {
       // stage 1 also evaluates the residual of y_n and runs the stop test
@@ -223,9 +225,13 @@ RelaxResult relax_loop(const Dims& d, RfmTables* rt, BcTables* bt, L2Tables* lt,
       a1.stall = w->stall;
       a1.stall_window = rp.stall_window;
       a1.stall_log_drop = rp.stall_log_drop;
+      a1.defer_l2 = 1;
       launch_substep<T>(1, a1);
-      for (int st = 2; st <= 4; st++)
+      launch_finalize_forked<T>(a1);  // the norm and stop test beside stage 2
+      for (int st = 2; st <= 4; st++) {
+        if (st == 3) join_finalize();
         launch_substep<T>(st, substep_args(d, rt, bt, s, b, rp, st, w->state + 1, w->state, tile));
+      }
     }
     NRPYELL_CUDA(cudaStreamEndCapture(stream(), &graph));
     set_launch_count(launches_before);  // captured launches count when the graph runs

@@ -42,6 +42,9 @@ struct SubstepArgs {
   double log10_tol;
   int max_steps;
   int check_every;  // 0: test every residual (main.c); > 0: the ET thorn's loop
+  // 1: the stage-1 blocks only store their per-tile partials and the norm
+  // and stop test are left to launch_finalize_forked (relaxation driver).
+  int defer_l2;
   // Optional stall test: stop (state[3] = 1) once the best log10 L2 so far
   // has not dropped by at least -stall_log_drop for stall_window steps;
   // stall[0..1] = best log10 L2 and the step it was reached.
@@ -75,6 +78,15 @@ template <typename T>
 void launch_columns_forked(int stage, const SubstepArgs& a);
 void join_columns();
 void prepare_columns();
+
+// Stop test of a stage-1 launch made with defer_l2 = 1: one block on
+// side_stream() sums the per-tile partials in index order and updates the
+// state (finalize_l2), beside the stage-2 launch; join_finalize() makes
+// stream() wait for it (before stage 3, the first launch that must see the
+// stop decision -- stage 4 writes y_n).
+template <typename T>
+void launch_finalize_forked(const SubstepArgs& a1);
+void join_finalize();
 
 // ---- marching variant (kernels_march.cu): shape v of the list there
 template <typename T>

@@ -472,7 +472,7 @@ __global__ void __launch_bounds__(32 * (NCW + 1), 1)
     // every consumer thread releases the stage after its last shared read
     mbar_arrive(&empty[s]);
     if (RESID) {
-      if (tile_partial<NCT, NamedSync<1, NCT>>(r2, tile, a.partials, a.ticket, a.n_tiles, sh, &last))
+      if (tile_partial<NCT, NamedSync<1, NCT>>(r2, tile, a.partials, a.ticket, a.n_tiles, sh, &last, a.defer_l2 != 0))
         finalize_l2<double, NCT, NamedSync<1, NCT>>(a, sh);
     }
   }

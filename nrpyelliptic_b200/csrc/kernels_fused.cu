@@ -109,7 +109,7 @@ __global__ void __launch_bounds__(32 * BY) k_substep(SubDev<T> a) {
       }
     }
   }
-  if (RESID && tile_partial<NT>(r2, b, a.partials, a.ticket, a.n_tiles, sh, &last)) finalize_l2<T, NT>(a, sh);
+  if (RESID && tile_partial<NT>(r2, b, a.partials, a.ticket, a.n_tiles, sh, &last, a.defer_l2 != 0)) finalize_l2<T, NT>(a, sh);
 }
 
 template <typename T, int STAGE>
@@ -255,7 +255,7 @@ __device__ __forceinline__ void planes_block(const SubDev<T>& a, int bid, double
       }
     }
   }
-  if (RESID && tile_partial<NT>(r2, b, a.partials, a.ticket, a.n_tiles, sh, &last)) finalize_l2<T, NT>(a, sh);
+  if (RESID && tile_partial<NT>(r2, b, a.partials, a.ticket, a.n_tiles, sh, &last, a.defer_l2 != 0)) finalize_l2<T, NT>(a, sh);
 }
 
 template <typename T, int STAGE, bool RESID, int BY, int P>
@@ -352,13 +352,15 @@ static void launch_planes(const SubstepArgs& a) {
   NRPYELL_LAUNCH((k_substep_planes<T, STAGE, RESID, BY, P>), f.n_tiles + f.n_col_blocks, NT, 0, f);
 }
 
-static cudaEvent_t g_fork = nullptr, g_join = nullptr;
+static cudaEvent_t g_fork = nullptr, g_join = nullptr, g_fin_fork = nullptr, g_fin_join = nullptr;
 
 void prepare_columns() {
   side_stream();
   if (!g_fork) {
     NRPYELL_CUDA(cudaEventCreateWithFlags(&g_fork, cudaEventDisableTiming));
     NRPYELL_CUDA(cudaEventCreateWithFlags(&g_join, cudaEventDisableTiming));
+    NRPYELL_CUDA(cudaEventCreateWithFlags(&g_fin_fork, cudaEventDisableTiming));
+    NRPYELL_CUDA(cudaEventCreateWithFlags(&g_fin_join, cudaEventDisableTiming));
   }
 }
 
@@ -385,6 +387,34 @@ void join_columns() {
   NRPYELL_CUDA(cudaEventRecord(g_join, side_stream()));
   NRPYELL_CUDA(cudaStreamWaitEvent(stream(), g_join, 0));
 }
+
+// The stop test of a deferred stage-1 launch (tile_partial with defer): one
+// block sums the per-tile partials in index order (finalize_l2).
+template <typename T>
+__global__ void __launch_bounds__(256) k_finalize_l2(SubDev<T> a) {
+  __shared__ double sh[8];
+  if (*a.done) return;
+  finalize_l2<T, 256>(a, sh);
+}
+
+template <typename T>
+void launch_finalize_forked(const SubstepArgs& a1) {
+  prepare_columns();
+  // the tile grid of the stage-1 launch: kind 3 runs the direct 32x4x2 shape
+  // where the bulk pipeline is unavailable
+  const TileShape s = kTiles[a1.tile];
+  const bool direct42 = s.kind == 3 && !bulk_available(a1, sizeof(T));
+  SubDev<T> f = make_dev<T>(a1, direct42 ? 4 : s.by, direct42 ? 2 : s.p);
+  cudaStream_t side = side_stream();
+  NRPYELL_CUDA(cudaEventRecord(g_fin_fork, stream()));
+  NRPYELL_CUDA(cudaStreamWaitEvent(side, g_fin_fork, 0));
+  NRPYELL_LAUNCH_ON(side, (k_finalize_l2<T>), 1, 256, 0, f);
+  NRPYELL_CUDA(cudaEventRecord(g_fin_join, side));
+}
+template void launch_finalize_forked<double>(const SubstepArgs&);
+template void launch_finalize_forked<float>(const SubstepArgs&);
+
+void join_finalize() { NRPYELL_CUDA(cudaStreamWaitEvent(stream(), g_fin_join, 0)); }
 
 template <typename T>
 void prepare_substep(int tile) {

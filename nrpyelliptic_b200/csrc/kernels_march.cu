@@ -198,7 +198,7 @@ __global__ void __launch_bounds__(32 * BY, MINB) k_substep_march(SubDev<T> a) {
       }
     }
   }
-  if (RESID && tile_partial<NT>(r2, b, a.partials, a.ticket, a.n_tiles, sh, &last)) finalize_l2<T, NT>(a, sh);
+  if (RESID && tile_partial<NT>(r2, b, a.partials, a.ticket, a.n_tiles, sh, &last, a.defer_l2 != 0)) finalize_l2<T, NT>(a, sh);
 }
 
 // Opts the kernel into more than 48 KB of dynamic shared memory, once per

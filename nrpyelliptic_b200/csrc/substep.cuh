@@ -37,6 +37,7 @@ struct SubDev {
   double volume, log10_tol;
   int max_steps;
   int check_every;  // > 0: Einstein Toolkit thorn semantics (see finalize_l2)
+  int defer_l2;     // stage 1: store the per-tile partials only (k_finalize_l2 reduces them)
   double* stall;
   int stall_window;
   double stall_log_drop;
@@ -222,10 +223,11 @@ __device__ void finalize_l2(const SubDev<T>& a, double* sh) {
 }
 
 // Reduces r2 over threads 0..NT-1, stores the tile's partial and returns
-// true in each of them if this tile was the last one to complete.
+// true in each of them if this tile was the last one to complete; with
+// `defer` it only stores the partial (a later launch reduces them).
 template <int NT, class Sync = BlockSync>
 __device__ __forceinline__ bool tile_partial(double r2, int tile, double* partials, unsigned int* ticket, int n_tiles,
-                                             double* sh, bool* last) {
+                                             double* sh, bool* last, bool defer = false) {
   const int tid = threadIdx.x;
 #pragma unroll
   for (int o = 16; o > 0; o >>= 1) r2 += __shfl_down_sync(0xffffffffu, r2, o);
@@ -235,11 +237,13 @@ __device__ __forceinline__ bool tile_partial(double r2, int tile, double* partia
     double t = 0.0;
     for (int wi = 0; wi < NT / 32; wi++) t += sh[wi];
     partials[tile] = t;
-    __threadfence();
-    *last = (atomicAdd(ticket, 1u) == (unsigned)n_tiles - 1);
+    if (!defer) {
+      __threadfence();
+      *last = (atomicAdd(ticket, 1u) == (unsigned)n_tiles - 1);
+    }
   }
   Sync::sync();
-  return *last;
+  return !defer && *last;
 }
 
 // ------------------------------------------------------------------ columns
@@ -539,6 +543,7 @@ inline SubDev<T> make_dev(const SubstepArgs& a, int by, int p) {
   f.log10_tol = a.log10_tol;
   f.max_steps = a.max_steps;
   f.check_every = a.check_every;
+  f.defer_l2 = a.defer_l2;
   f.stall = a.stall;
   f.stall_window = a.stall_window;
   f.stall_log_drop = a.stall_log_drop;
