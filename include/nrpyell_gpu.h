@@ -236,7 +236,9 @@ int nrpyell_interpolate_solution(const paramstruct *params, REAL *xx[3], const R
  * nrpyell_relax (its own grid size, parameters, bc_struct, rfm_struct and
  * device gridfunctions; dt[c] its time step), relaxed together from their
  * y_n_gfs to log10 L2 <= log10_tol or max_steps.  Every RK4 substep of all
- * configurations is one kernel launch; each configuration stops on its own.
+ * configurations is one kernel launch (a shared-memory planes or marching
+ * shape, autotuned on the batch or forced by nrpyell_set_tile); each
+ * configuration stops on its own.
  * steps_taken[c] and final_log10_l2[c] as in nrpyell_relax.  Returns the
  * number of configurations that did not converge (0: all did), < 0 on
  * error. */

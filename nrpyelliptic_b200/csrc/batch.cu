@@ -1,6 +1,7 @@
 // Batched relaxation: many puncture configurations, on grids of different
 // sizes, relaxed together.  Every RK4 substep of all configurations is one
-// launch of the shared-memory planes kernel (k_substep_planes_batch): the
+// launch of the shared-memory planes or marching kernel
+// (k_substep_planes_batch, k_substep_march_batch): the
 // launch's blocks are the concatenated column blocks and interior tiles of
 // all grids, and each grid keeps its own launch arguments, stop test and
 // done flag, so a grid that has converged costs one flag read per block.
@@ -98,7 +99,7 @@ bool build_devs(const std::vector<Grid>& grids, int tile, std::vector<SubDev<dou
         a.stall = g_batch.stall + 2 * c;
         a.stall_window = 0;
       }
-      if (!planes_launch_dev<double>(a, &(*devs)[k * n + c])) return false;
+      if (!batch_launch_dev<double>(a, &(*devs)[k * n + c])) return false;
     }
     const SubDev<double>& f = (*devs)[c];
     if (f.n_tiles > g_batch.partials_per) {
@@ -120,11 +121,11 @@ bool upload_devs(const std::vector<SubDev<double>>& devs, const std::vector<int>
   return status_ok();
 }
 
-// Shared-memory planes shapes of the tile table.
-std::vector<int> planes_tiles() {
+// Shared-memory planes and marching shapes of the tile table.
+std::vector<int> batch_tiles() {
   std::vector<int> t;
   for (int i = 0; i < substep_num_tiles(); i++)
-    if (substep_tile_kind(i) == 4) t.push_back(i);
+    if (substep_tile_kind(i) == 4 || substep_tile_kind(i) == 5) t.push_back(i);
   return t;
 }
 
@@ -173,10 +174,11 @@ extern "C" int nrpyell_relax_batch(const int n, griddata_struct* grids, const RE
   }
   if (!ensure_batch(n, max_steps + 1, max_tiles)) return -1;
 
-  // tile shape: forced planes shape, else the fastest on this batch
-  const std::vector<int> cands = planes_tiles();
+  // tile shape: forced planes or marching shape, else the fastest on this batch
+  const std::vector<int> cands = batch_tiles();
   int tile = -1;
-  if (g_forced_tile >= 0 && substep_tile_kind(g_forced_tile) == 4) tile = g_forced_tile;
+  if (g_forced_tile >= 0 && (substep_tile_kind(g_forced_tile) == 4 || substep_tile_kind(g_forced_tile) == 5))
+    tile = g_forced_tile;
   std::vector<SubDev<double>> devs;
   std::vector<int> offs;
   int blocks = 0;

@@ -487,17 +487,17 @@ template void launch_substep<float>(int, const SubstepArgs&);
 // ---------------------------------------------------------------- batches
 
 template <typename T>
-bool planes_launch_dev(const SubstepArgs& a, SubDev<T>* out) {
+bool batch_launch_dev(const SubstepArgs& a, SubDev<T>* out) {
   const int t = a.tile;
-  if (t < 0 || t >= kNumTiles || kTiles[t].kind != 4) {
-    NRPYELL_FAIL("batched substep: the tile must be a shared-memory planes shape");
+  if (t < 0 || t >= kNumTiles || (kTiles[t].kind != 4 && kTiles[t].kind != 5)) {
+    NRPYELL_FAIL("batched substep: the tile must be a shared-memory planes or marching shape");
     return false;
   }
   *out = make_dev<T>(a, kTiles[t].by, kTiles[t].p);
   out->n_col_blocks = ((a.d.Nxx1 + kRows - 1) / kRows) * a.d.Nxx2;
   return true;
 }
-template bool planes_launch_dev<double>(const SubstepArgs&, SubDev<double>*);
+template bool batch_launch_dev<double>(const SubstepArgs&, SubDev<double>*);
 
 template <typename T, int STAGE, bool RESID>
 static void launch_batch_stage(int tile, const SubDev<T>* devs, const int* offs, int n, int blocks) {
@@ -521,6 +521,10 @@ static void launch_batch_stage(int tile, const SubDev<T>* devs, const int* offs,
 template <typename T>
 void launch_substep_batch(int stage, bool resid, int tile, const SubDev<T>* devs, const int* offs, int n,
                           int blocks) {
+  if (kTiles[tile].kind == 5) {
+    launch_march_batch<T>(stage, resid, kTiles[tile].v, devs, offs, n, blocks);
+    return;
+  }
   switch (stage) {
     case 1:
       if (resid)

@@ -59,15 +59,12 @@ struct MarchSmem {
   static constexpr size_t bytes = march > sizeof(double) * kRowsSmem ? march : sizeof(double) * kRowsSmem;
 };
 
-template <typename T, int STAGE, bool RESID, int BY, int PZ, int D, int MINB>
-__global__ void __launch_bounds__(32 * BY, MINB) k_substep_march(SubDev<T> a) {
-  extern __shared__ __align__(16) double dsm[];
-  __shared__ double sh[BY > 8 ? BY : 8];
-  __shared__ bool last;
-  if (*a.done) return;
+// Block `bid` of one grid's marching launch (column blocks first); dsm is
+// the block's dynamic shared memory (MarchSmem::bytes).
+template <typename T, int STAGE, bool RESID, int BY, int PZ, int D>
+__device__ __forceinline__ void march_block(const SubDev<T>& a, const int bid, double* dsm, double* sh, bool* lastp) {
   using L = MarchSmem<T, BY, STAGE, D>;
   constexpr int NT = L::NT, NR = L::NR, RWS = L::RWS, HALF = RWS / 2;
-  const int bid = blockIdx.x;
   if (bid < a.n_col_blocks) {
     column_rows<T, STAGE, NT>(a, bid, dsm);
     return;
@@ -198,12 +195,45 @@ __global__ void __launch_bounds__(32 * BY, MINB) k_substep_march(SubDev<T> a) {
       }
     }
   }
-  if (RESID && tile_partial<NT>(r2, b, a.partials, a.ticket, a.n_tiles, sh, &last, a.defer_l2 != 0)) finalize_l2<T, NT>(a, sh);
+  if (RESID && tile_partial<NT>(r2, b, a.partials, a.ticket, a.n_tiles, sh, lastp, a.defer_l2 != 0))
+    finalize_l2<T, NT>(a, sh);
+}
+
+template <typename T, int STAGE, bool RESID, int BY, int PZ, int D, int MINB>
+__global__ void __launch_bounds__(32 * BY, MINB) k_substep_march(SubDev<T> a) {
+  extern __shared__ __align__(16) double dsm[];
+  __shared__ double sh[BY > 8 ? BY : 8];
+  __shared__ bool last;
+  if (*a.done) return;
+  march_block<T, STAGE, RESID, BY, PZ, D>(a, blockIdx.x, dsm, sh, &last);
+}
+
+// One substep of many grids in one launch: the blocks of grid c are
+// offs[c] .. offs[c+1]-1 (column blocks first, then interior tiles), each
+// grid with its own launch arguments, stop test and done flag.
+template <typename T, int STAGE, bool RESID, int BY, int PZ, int D, int MINB>
+__global__ void __launch_bounds__(32 * BY, MINB)
+    k_substep_march_batch(const SubDev<T>* __restrict__ devs, const int* __restrict__ offs, int n) {
+  extern __shared__ __align__(16) double dsm[];
+  __shared__ double sh[BY > 8 ? BY : 8];
+  __shared__ bool last;
+  int lo = 0, hi = n - 1;
+  const int bx = blockIdx.x;
+  while (lo < hi) {
+    const int mid = (lo + hi + 1) >> 1;
+    if (__ldg(offs + mid) <= bx)
+      lo = mid;
+    else
+      hi = mid - 1;
+  }
+  const SubDev<T>& a = devs[lo];
+  if (*a.done) return;
+  march_block<T, STAGE, RESID, BY, PZ, D>(a, bx - __ldg(offs + lo), dsm, sh, &last);
 }
 
 // Opts the kernel into more than 48 KB of dynamic shared memory, once per
 // device.
-template <typename T, int STAGE, bool RESID, int BY, int PZ, int D, int MINB>
+template <typename T, int STAGE, bool RESID, int BY, int PZ, int D, int MINB, bool BATCH = false>
 bool march_opt_in() {
   static unsigned long long devices = 0;
   const size_t bytes = MarchSmem<T, BY, STAGE, D>::bytes;
@@ -211,8 +241,12 @@ bool march_opt_in() {
   int dev = 0;
   NRPYELL_CUDA(cudaGetDevice(&dev));
   if (dev >= 0 && dev < 64 && !(devices >> dev & 1ull)) {
-    NRPYELL_CUDA(cudaFuncSetAttribute(k_substep_march<T, STAGE, RESID, BY, PZ, D, MINB>,
-                                      cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes));
+    if constexpr (BATCH)
+      NRPYELL_CUDA(cudaFuncSetAttribute(k_substep_march_batch<T, STAGE, RESID, BY, PZ, D, MINB>,
+                                        cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes));
+    else
+      NRPYELL_CUDA(cudaFuncSetAttribute(k_substep_march<T, STAGE, RESID, BY, PZ, D, MINB>,
+                                        cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes));
     devices |= 1ull << dev;
   }
   return status_ok();
@@ -239,6 +273,26 @@ bool march_stage(int v, const SubstepArgs& a) {
 #define NRPYELL_MARCH(I, BY, PZ, D, MINB)                          \
   case I:                                                          \
     launch_march_shape<T, STAGE, RESID, BY, PZ, D, MINB>(a);       \
+    return true;
+    NRPYELL_MARCH_SHAPES(NRPYELL_MARCH)
+#undef NRPYELL_MARCH
+  }
+  return false;
+}
+
+template <typename T, int STAGE, bool RESID, int BY, int PZ, int D, int MINB>
+void launch_march_batch_shape(const SubDev<T>* devs, const int* offs, int n, int blocks) {
+  if (!march_opt_in<T, STAGE, RESID, BY, PZ, D, MINB, true>()) return;
+  NRPYELL_LAUNCH((k_substep_march_batch<T, STAGE, RESID, BY, PZ, D, MINB>), blocks, 32 * BY,
+                 (MarchSmem<T, BY, STAGE, D>::bytes), devs, offs, n);
+}
+
+template <typename T, int STAGE, bool RESID>
+bool march_batch_stage(int v, const SubDev<T>* devs, const int* offs, int n, int blocks) {
+  switch (v) {
+#define NRPYELL_MARCH(I, BY, PZ, D, MINB)                                           \
+  case I:                                                                           \
+    launch_march_batch_shape<T, STAGE, RESID, BY, PZ, D, MINB>(devs, offs, n, blocks); \
     return true;
     NRPYELL_MARCH_SHAPES(NRPYELL_MARCH)
 #undef NRPYELL_MARCH
@@ -282,5 +336,21 @@ void prepare_march(int v) {
 }
 template void prepare_march<double>(int);
 template void prepare_march<float>(int);
+
+template <typename T>
+void launch_march_batch(int stage, bool resid, int v, const SubDev<T>* devs, const int* offs, int n, int blocks) {
+  bool ok = false;
+  switch (stage) {
+    case 1:
+      ok = resid ? march_batch_stage<T, 1, true>(v, devs, offs, n, blocks)
+                 : march_batch_stage<T, 1, false>(v, devs, offs, n, blocks);
+      break;
+    case 2: ok = march_batch_stage<T, 2, false>(v, devs, offs, n, blocks); break;
+    case 3: ok = march_batch_stage<T, 3, false>(v, devs, offs, n, blocks); break;
+    default: ok = march_batch_stage<T, 4, false>(v, devs, offs, n, blocks); break;
+  }
+  if (!ok) NRPYELL_FAIL("launch_march_batch: no kernel for this shape");
+}
+template void launch_march_batch<double>(int, bool, int, const SubDev<double>*, const int*, int, int);
 
 }  // namespace nrpyell

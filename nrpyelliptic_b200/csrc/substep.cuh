@@ -497,16 +497,19 @@ __device__ __forceinline__ int wrapm(int j, int Nxx2) {
 template <typename T>
 inline SubDev<T> make_dev(const SubstepArgs& a, int by, int p);
 
-// ---- batched launches (kernels_fused.cu): the shared-memory planes kernel
-// over many grids in one launch.
-// Launch arguments of one grid for the planes shape a.tile (kind 4).
+// ---- batched launches (kernels_fused.cu, kernels_march.cu): the
+// shared-memory planes or marching kernel over many grids in one launch.
+// Launch arguments of one grid for the shape a.tile (kind 4 or 5).
 template <typename T>
-bool planes_launch_dev(const SubstepArgs& a, SubDev<T>* out);
+bool batch_launch_dev(const SubstepArgs& a, SubDev<T>* out);
 // One substep of n grids; devs (device) holds the grids' arguments for this
 // stage, offs (device) their first block; blocks = total blocks.
 template <typename T>
 void launch_substep_batch(int stage, bool resid, int tile, const SubDev<T>* devs, const int* offs, int n,
                           int blocks);
+// The marching kernel's part of launch_substep_batch: shape v of its list.
+template <typename T>
+void launch_march_batch(int stage, bool resid, int v, const SubDev<T>* devs, const int* offs, int n, int blocks);
 
 template <typename T>
 inline SubDev<T> make_dev(const SubstepArgs& a, int by, int p) {

@@ -14,6 +14,7 @@ from nrpyelliptic_b200.problem import CONFIGS, DeviceState, Problem, sample_swee
 
 pytestmark = pytest.mark.gpu
 PLANES_8x1 = 20  # a shared-memory planes tile shape (kind 4)
+MARCH_8x4 = 25  # a marching tile shape (kind 5)
 
 
 @pytest.fixture(scope="module")
@@ -36,11 +37,14 @@ def _alone(lib, prob, max_steps):
     return rc, steps.value, fin.value, y
 
 
-def test_batch_matches_single_runs(lib):
+@pytest.mark.parametrize("tile", [PLANES_8x1, MARCH_8x4])
+def test_batch_matches_single_runs(lib, tile):
+    kind = C.c_int(-1)
+    assert lib.nrpyell_tile_info(tile, None, None, C.byref(kind)) == 0 and kind.value in (4, 5)
     cfgs = [CONFIGS["shipped_64x64x8"], with_grid(CONFIGS["quasicircular_128x128x16"], (48, 48, 8)),
             with_grid(sample_sweep(4)[1], (40, 24, 6)), CONFIGS["equal_mass_rest_64x64x8"]]
     probs = [Problem(c, lib=lib) for c in cfgs]
-    lib.nrpyell_set_tile(PLANES_8x1)
+    lib.nrpyell_set_tile(tile)
     try:
         rc, steps, finals, states = relax_batch(probs, tol=-10.0, max_steps=8000, lib=lib)
         assert rc == 0
