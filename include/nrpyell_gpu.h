@@ -136,6 +136,14 @@ void nrpyell_set_async(int enable);
  * and its pointwise inputs copied into shared memory ahead of use by
  * asynchronous copies. */
 void nrpyell_set_tile(int tile);
+/* Programmatic dependent launch of the fused substep kernels (default on):
+ * each substep kernel may be scheduled while the previous one drains and
+ * waits on the device (griddepcontrol.wait) before reading its results, so
+ * the launch gap between the four substeps of an RK4 step is hidden.  Results
+ * are identical either way; 0 turns it off (cached relaxation graphs are
+ * dropped and captured again). */
+void nrpyell_set_programmatic_launch(int on);
+int nrpyell_get_programmatic_launch(void);
 int nrpyell_get_tile(const paramstruct *params, int fp32, int *bx, int *by, int *planes);
 int nrpyell_num_tiles(void);
 int nrpyell_tile_info(int tile, int *by, int *planes, int *kind);

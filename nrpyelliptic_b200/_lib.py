@@ -44,6 +44,8 @@ EXPORTS = {
     "nrpyell_set_device": (C.c_int, [C.c_int]),
     "nrpyell_set_async": (None, [C.c_int]),
     "nrpyell_set_tile": (None, [C.c_int]),
+    "nrpyell_set_programmatic_launch": (None, [C.c_int]),
+    "nrpyell_get_programmatic_launch": (C.c_int, []),
     "nrpyell_get_tile": (C.c_int, [P(abi.paramstruct), C.c_int, P(C.c_int), P(C.c_int), P(C.c_int)]),
     "nrpyell_num_tiles": (C.c_int, []),
     "nrpyell_tile_info": (C.c_int, [C.c_int, P(C.c_int), P(C.c_int), P(C.c_int)]),

@@ -240,6 +240,14 @@ void nrpyell_set_async(int enable) { g_async = enable != 0; }
 
 void nrpyell_set_tile(int tile) { g_forced_tile = (tile >= 0 && tile < substep_num_tiles()) ? tile : -1; }
 
+void nrpyell_set_programmatic_launch(int on) {
+  if (g_pdl == (on != 0)) return;
+  if (g_stream) NRPYELL_CUDA(cudaStreamSynchronize(g_stream));
+  release_graphs();  // cached relaxation graphs were captured with the other setting
+  g_pdl = on != 0;
+}
+int nrpyell_get_programmatic_launch(void) { return g_pdl ? 1 : 0; }
+
 int nrpyell_get_tile(const paramstruct* params, int fp32, int* bx, int* by, int* planes) {
   int tile = g_forced_tile >= 0 ? g_forced_tile : find_tile(dims_of(params), fp32);
   if (tile >= 0 && bx && by && planes) substep_tile_shape(tile, bx, by, planes);

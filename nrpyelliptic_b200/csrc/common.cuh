@@ -5,6 +5,8 @@
 #include <stdint.h>
 #include <stdio.h>
 
+#include <utility>
+
 #include "nrpyell_gpu.h"
 
 namespace nrpyell {
@@ -49,6 +51,38 @@ void set_launch_count(long long n);
     kernel<<<(grid), (block), (smem), (strm)>>>(__VA_ARGS__);                  \
     ::nrpyell::count_launch();                                                 \
     NRPYELL_CUDA(cudaGetLastError());                                          \
+  } while (0)
+
+// Programmatic dependent launch of the fused substep kernels (on unless
+// nrpyell_set_programmatic_launch(0)): a kernel launched this way may be
+// scheduled while the previous kernel of the stream drains, and waits in
+// griddepcontrol.wait (pdl_enter) before it touches that kernel's results.
+bool pdl_enabled();
+
+template <typename... KArgs, typename... Args>
+inline cudaError_t launch_maybe_pdl(void (*kern)(KArgs...), dim3 grid, dim3 block, size_t smem, cudaStream_t s,
+                                    Args&&... args) {
+  if (!pdl_enabled()) {
+    kern<<<grid, block, smem, s>>>(std::forward<Args>(args)...);
+    return cudaGetLastError();
+  }
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = grid;
+  cfg.blockDim = block;
+  cfg.dynamicSmemBytes = smem;
+  cfg.stream = s;
+  cudaLaunchAttribute attr[1];
+  attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+  attr[0].val.programmaticStreamSerializationAllowed = 1;
+  cfg.attrs = attr;
+  cfg.numAttrs = 1;
+  return cudaLaunchKernelEx(&cfg, kern, std::forward<Args>(args)...);
+}
+#define NRPYELL_LAUNCH_PDL(kernel, grid, block, smem, ...)                                                     \
+  do {                                                                                                         \
+    NRPYELL_CUDA(::nrpyell::launch_maybe_pdl(kernel, dim3(grid), dim3(block), (smem), ::nrpyell::stream(),     \
+                                             __VA_ARGS__));                                                    \
+    ::nrpyell::count_launch();                                                                                 \
   } while (0)
 
 // Grid geometry passed by value to kernels.

@@ -10,6 +10,8 @@
 namespace nrpyell {
 
 int g_forced_tile = -1;
+bool g_pdl = true;
+bool pdl_enabled() { return g_pdl; }
 int g_work_generation = 0;
 static std::vector<FusedWork*> g_work;
 

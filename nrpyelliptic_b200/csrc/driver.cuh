@@ -47,6 +47,7 @@ struct RelaxResult {
 };
 
 extern int g_forced_tile;
+extern bool g_pdl;  // programmatic dependent launch of the substep kernels
 extern int g_work_generation;
 
 FusedWork* get_work(const Dims& d, int history_len);

@@ -37,6 +37,7 @@ __global__ void __launch_bounds__(32 * BY) k_substep(SubDev<T> a) {
   constexpr int NT = 32 * BY;
   __shared__ double sh[NT / 32 > 8 ? NT / 32 : 8];
   __shared__ bool last;
+  pdl_enter();
   if (*a.done) return;
   if ((int)blockIdx.x < a.n_col_blocks) {
     column_block<T, STAGE, NT>(a, blockIdx.x);
@@ -263,6 +264,7 @@ __global__ void __launch_bounds__(32 * BY) k_substep_planes(SubDev<T> a) {
   __shared__ double smem[PlanesSmem<T, BY, P>::value];
   __shared__ double sh[BY > 8 ? BY : 8];
   __shared__ bool last;
+  pdl_enter();
   if (*a.done) return;
   planes_block<T, STAGE, RESID, BY, P>(a, blockIdx.x, smem, sh, &last);
 }
@@ -276,6 +278,7 @@ __global__ void __launch_bounds__(32 * BY)
   __shared__ double smem[PlanesSmem<T, BY, P>::value];
   __shared__ double sh[BY > 8 ? BY : 8];
   __shared__ bool last;
+  pdl_enter();
   int lo = 0, hi = n - 1;
   const int bx = blockIdx.x;
   while (lo < hi) {
@@ -341,7 +344,7 @@ static void launch_direct(const SubstepArgs& a) {
   constexpr int NT = 32 * BY;
   constexpr int CB = NT / kColThreadsPerColumn;
   f.n_col_blocks = (f.ncol + CB - 1) / CB;
-  NRPYELL_LAUNCH((k_substep<T, STAGE, RESID, BY, P, PF>), f.n_tiles + f.n_col_blocks, NT, 0, f);
+  NRPYELL_LAUNCH_PDL((k_substep<T, STAGE, RESID, BY, P, PF>), f.n_tiles + f.n_col_blocks, NT, 0, f);
 }
 
 template <typename T, int STAGE, bool RESID, int BY, int P>
@@ -349,7 +352,7 @@ static void launch_planes(const SubstepArgs& a) {
   SubDev<T> f = make_dev<T>(a, BY, P);
   constexpr int NT = 32 * BY;
   f.n_col_blocks = ((a.d.Nxx1 + kRows - 1) / kRows) * a.d.Nxx2;
-  NRPYELL_LAUNCH((k_substep_planes<T, STAGE, RESID, BY, P>), f.n_tiles + f.n_col_blocks, NT, 0, f);
+  NRPYELL_LAUNCH_PDL((k_substep_planes<T, STAGE, RESID, BY, P>), f.n_tiles + f.n_col_blocks, NT, 0, f);
 }
 
 static cudaEvent_t g_fork = nullptr, g_join = nullptr, g_fin_fork = nullptr, g_fin_join = nullptr;
@@ -504,7 +507,7 @@ static void launch_batch_stage(int tile, const SubDev<T>* devs, const int* offs,
   const int by = kTiles[tile].by, p = kTiles[tile].p;
 #define NRPYELL_BATCH(BY, P)                                                                           \
   if (by == BY && p == P) {                                                                            \
-    NRPYELL_LAUNCH((k_substep_planes_batch<T, STAGE, RESID, BY, P>), blocks, 32 * BY, 0, devs, offs, n); \
+    NRPYELL_LAUNCH_PDL((k_substep_planes_batch<T, STAGE, RESID, BY, P>), blocks, 32 * BY, 0, devs, offs, n); \
     return;                                                                                            \
   }
   NRPYELL_BATCH(4, 2)

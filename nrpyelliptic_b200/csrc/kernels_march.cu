@@ -204,6 +204,7 @@ __global__ void __launch_bounds__(32 * BY, MINB) k_substep_march(SubDev<T> a) {
   extern __shared__ __align__(16) double dsm[];
   __shared__ double sh[BY > 8 ? BY : 8];
   __shared__ bool last;
+  pdl_enter();
   if (*a.done) return;
   march_block<T, STAGE, RESID, BY, PZ, D>(a, blockIdx.x, dsm, sh, &last);
 }
@@ -217,6 +218,7 @@ __global__ void __launch_bounds__(32 * BY, MINB)
   extern __shared__ __align__(16) double dsm[];
   __shared__ double sh[BY > 8 ? BY : 8];
   __shared__ bool last;
+  pdl_enter();
   int lo = 0, hi = n - 1;
   const int bx = blockIdx.x;
   while (lo < hi) {
@@ -257,8 +259,8 @@ void launch_march_shape(const SubstepArgs& a) {
   if (!march_opt_in<T, STAGE, RESID, BY, PZ, D, MINB>()) return;
   SubDev<T> f = make_dev<T>(a, BY, PZ);
   f.n_col_blocks = ((a.d.Nxx1 + kRows - 1) / kRows) * a.d.Nxx2;
-  NRPYELL_LAUNCH((k_substep_march<T, STAGE, RESID, BY, PZ, D, MINB>), f.n_tiles + f.n_col_blocks, 32 * BY,
-                 (MarchSmem<T, BY, STAGE, D>::bytes), f);
+  NRPYELL_LAUNCH_PDL((k_substep_march<T, STAGE, RESID, BY, PZ, D, MINB>), f.n_tiles + f.n_col_blocks, 32 * BY,
+                     (MarchSmem<T, BY, STAGE, D>::bytes), f);
 }
 
 // The compiled shapes, by index: (BY, PZ, ring slots D, minimum resident
@@ -283,8 +285,8 @@ bool march_stage(int v, const SubstepArgs& a) {
 template <typename T, int STAGE, bool RESID, int BY, int PZ, int D, int MINB>
 void launch_march_batch_shape(const SubDev<T>* devs, const int* offs, int n, int blocks) {
   if (!march_opt_in<T, STAGE, RESID, BY, PZ, D, MINB, true>()) return;
-  NRPYELL_LAUNCH((k_substep_march_batch<T, STAGE, RESID, BY, PZ, D, MINB>), blocks, 32 * BY,
-                 (MarchSmem<T, BY, STAGE, D>::bytes), devs, offs, n);
+  NRPYELL_LAUNCH_PDL((k_substep_march_batch<T, STAGE, RESID, BY, PZ, D, MINB>), blocks, 32 * BY,
+                     (MarchSmem<T, BY, STAGE, D>::bytes), devs, offs, n);
 }
 
 template <typename T, int STAGE, bool RESID>

@@ -46,6 +46,16 @@ struct SubDev {
   double invdx0, invdx1;
 };
 
+// Entry of a substep kernel: waits until the kernels before it in the
+// stream have completed and their writes are visible (a no-op unless it was
+// launched with programmatic stream serialization), then lets the next
+// kernel's blocks be scheduled as this grid drains.  Nothing written by an
+// earlier kernel -- the state, the done flag -- is read before it.
+__device__ __forceinline__ void pdl_enter() {
+  asm volatile("griddepcontrol.wait;\n" ::: "memory");
+  asm volatile("griddepcontrol.launch_dependents;\n" ::: "memory");
+}
+
 // Interior index along i2 after a wrap by 2 pi.
 __device__ __forceinline__ int wrap2(int j, int Nxx2) {
   j -= NGHOSTS;

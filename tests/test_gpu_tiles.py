@@ -122,3 +122,29 @@ def test_shared_memory_tiles_in_mixed_precision(lib):
             ds.free()
     finally:
         lib.nrpyell_set_tile(-1)
+
+
+def test_programmatic_launch_gives_identical_relaxations(lib):
+    """The substep kernels launched with programmatic stream serialization
+    (each waits in griddepcontrol.wait for the previous substep) and launched
+    plainly give the same relaxation, bit for bit."""
+    prob = Problem(CONFIGS["shipped_64x64x8"])
+    out = {}
+    try:
+        for on in (1, 0):
+            lib.nrpyell_set_programmatic_launch(on)
+            assert lib.nrpyell_get_programmatic_launch() == on
+            ds = DeviceState(prob)
+            steps, fin = C.c_int(0), C.c_double(0)
+            hist = np.zeros(4001)
+            rc = lib.nrpyell_relax(C.byref(ds.g), prob.dt, -10.0, 4000, 100.0, C.byref(steps), C.byref(fin),
+                                   ptr(hist))
+            _lib.check(lib)
+            assert rc == 0
+            out[on] = (steps.value, fin.value, hist.copy(), ds.download("y_n"))
+            ds.free()
+    finally:
+        lib.nrpyell_set_programmatic_launch(1)
+    assert out[1][0] == out[0][0] and out[1][1] == out[0][1]
+    np.testing.assert_array_equal(out[1][2], out[0][2])
+    np.testing.assert_array_equal(out[1][3], out[0][3])
