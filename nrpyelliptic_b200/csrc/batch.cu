@@ -175,7 +175,11 @@ extern "C" int nrpyell_relax_batch(const int n, griddata_struct* grids, const RE
   if (!ensure_batch(n, max_steps + 1, max_tiles)) return -1;
 
   // tile shape: forced planes or marching shape, else the fastest on this batch
-  const std::vector<int> cands = batch_tiles();
+  bool fits = true;
+  for (const Grid& G : gs) fits = fits && march_fits(G.d);
+  std::vector<int> cands;
+  for (int t : batch_tiles())
+    if (fits || substep_tile_kind(t) != 5) cands.push_back(t);
   int tile = -1;
   if (g_forced_tile >= 0 && (substep_tile_kind(g_forced_tile) == 4 || substep_tile_kind(g_forced_tile) == 5))
     tile = g_forced_tile;

@@ -88,9 +88,12 @@ template <typename T>
 void launch_finalize_forked(const SubstepArgs& a1);
 void join_finalize();
 
-// ---- marching variant (kernels_march.cu): shape v of the list there
+// ---- marching variant (kernels_march.cu): shape v of the list there.  Its
+// element offsets are 32-bit: grids with 3 Ntot >= 2^32 do not fit
+// (launch_march returns false and launches nothing).
+bool march_fits(const Dims& d);
 template <typename T>
-void launch_march(int stage, bool resid, int v, const SubstepArgs& a);
+bool launch_march(int stage, bool resid, int v, const SubstepArgs& a);
 // Shared-memory opt-in of a shape's kernels (before a stream capture).
 template <typename T>
 void prepare_march(int v);

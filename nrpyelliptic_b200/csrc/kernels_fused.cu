@@ -46,63 +46,101 @@ __global__ void __launch_bounds__(32 * BY) k_substep(SubDev<T> a) {
   const int tid = threadIdx.x;
   const int b = blockIdx.x - a.n_col_blocks;
   const int t0 = b % a.tiles0, t1 = (b / a.tiles0) % a.tiles1, t2 = b / (a.tiles0 * a.tiles1);
+  const int i10 = t1 * BY + NGHOSTS;
   const int i0 = t0 * 32 + (tid & 31) + NGHOSTS;
-  const int i1 = t1 * BY + (tid >> 5) + NGHOSTS;
+  const int i1 = i10 + (tid >> 5);
   const int z0 = t2 * P + NGHOSTS;
+  const int N0 = a.N0, top = NGHOSTS + a.Nxx1, Nxx2 = a.Nxx2;
+  // element offsets fit in 32 bits (the launcher checks march_fits)
+  const unsigned N01 = (unsigned)a.N01, Ntot = (unsigned)a.Ntot;
+  const bool once = Nxx2 >= 2 * NGHOSTS;  // i2 indices below wrap at most once
+  auto wrapz = [&](int j) -> int {
+    if (once) return j < NGHOSTS ? j + Nxx2 : (j >= NGHOSTS + Nxx2 ? j - Nxx2 : j);
+    return wrapm(j, Nxx2);
+  };
+  // the i0/i1 arms of every point of this tile stay off the inner ghost zones
+  const bool clear = t0 > 0 && i10 >= 2 * NGHOSTS && i10 + BY + NGHOSTS <= top;
   double r2 = 0.0;
-  if (i0 < NGHOSTS + a.Nxx0 && i1 < NGHOSTS + a.Nxx1) {
-    const T* u = a.S;
-    const long long line = i0 + (long long)a.N0 * i1;
-    const long long Ntot = a.Ntot;
+  if (i0 < NGHOSTS + a.Nxx0 && i1 < top) {
+    const T* __restrict__ u = a.S;
+    const unsigned k2 = (unsigned)(i0 + N0 * i1);
     // uu along i2 for planes z0-5 .. z0+P+4 (wrapped by 2 pi)
     T col[P + 10];
 #pragma unroll
-    for (int q = 0; q < P + 10; q++) col[q] = __ldg(u + line + a.N01 * wrap2(z0 - 5 + q, a.Nxx2));
+    for (int q = 0; q < P + 10; q++) col[q] = __ldg(u + (k2 + N01 * (unsigned)wrapz(z0 - 5 + q)));
     // PF: every pointwise input of the P planes is loaded before the first
     // store (the stores may alias y_n, so the compiler cannot hoist them).
     T pf[8][P];  // unused (and removed) when !PF
     if (PF) {
 #pragma unroll
       for (int p = 0; p < P; p++) {
-        const long long idx = line + a.N01 * (z0 + p < NGHOSTS + a.Nxx2 ? z0 + p : z0);
-        pf[0][p] = __ldg(a.S + Ntot + idx);
-        pf[1][p] = __ldg(a.aux + ADD_TIMES_AUUGF * Ntot + idx);
-        pf[2][p] = __ldg(a.aux + PSI_BACKGROUNDGF * Ntot + idx);
-        pf[3][p] = __ldg(a.aux + WAVESPEEDGF * Ntot + idx);
+        const unsigned idx = k2 + N01 * (unsigned)(z0 + p < NGHOSTS + Nxx2 ? z0 + p : z0);
+        pf[0][p] = __ldg(a.S + (idx + Ntot));
+        pf[1][p] = __ldg(a.aux + (idx + ADD_TIMES_AUUGF * Ntot));
+        pf[2][p] = __ldg(a.aux + (idx + PSI_BACKGROUNDGF * Ntot));
+        pf[3][p] = __ldg(a.aux + (idx + WAVESPEEDGF * Ntot));
         pf[4][p] = a.y[idx];
-        pf[5][p] = a.y[Ntot + idx];
+        pf[5][p] = a.y[idx + Ntot];
         pf[6][p] = (STAGE == 1) ? (T)0 : a.acc[idx];
-        pf[7][p] = (STAGE == 1) ? (T)0 : a.acc[Ntot + idx];
+        pf[7][p] = (STAGE == 1) ? (T)0 : a.acc[idx + Ntot];
       }
     }
-    const int k2 = i0 + a.N0 * i1;
 #pragma unroll
     for (int p = 0; p < P; p++) {
       const int i2 = z0 + p;
-      if (i2 < NGHOSTS + a.Nxx2) {
-        const int i2h = wrap2(i2 + a.half2, a.Nxx2);
+      if (i2 < NGHOSTS + Nxx2) {
+        const unsigned idx = k2 + N01 * (unsigned)i2;
         T s0 = 0, s1 = 0, s00 = 0, s11 = 0, s22 = 0;
-        stencil01<T>(a, u, i0, i1, i2, i2h, s0, s1, s00, s11);
+        if (clear) {
+          // the star's i0/i1 arms at fixed offsets from the point
+          const T* pc = u + idx;
+#pragma unroll
+          for (int k = 1; k <= 5; k++) {
+            const T am = __ldg(pc - k), ap = __ldg(pc + k);
+            const T bm = __ldg(pc - k * N0), bp = __ldg(pc + k * N0);
+            s0 = fma(W<T>::d(k), ap - am, s0);
+            s1 = fma(W<T>::d(k), bp - bm, s1);
+            s00 = fma(W<T>::e(k), ap + am, s00);
+            s11 = fma(W<T>::e(k), bp + bm, s11);
+          }
+        } else {
+          stencil01<T>(a, u, i0, i1, i2, wrap2(i2 + a.half2, Nxx2), s0, s1, s00, s11);
+        }
 #pragma unroll
         for (int k = 1; k <= 5; k++) s22 = fma(W<T>::e(k), col[p + 5 + k] + col[p + 5 - k], s22);
-        const long long idx = line + a.N01 * i2;
         T ku, kv, br;
+        T yu, yv, accu, accv;
+        // the six metric weights, loaded per plane (cached in L1; holding
+        // them in registers across the planes costs occupancy)
+        const T C22 = __ldg(a.coef + k2), C00 = __ldg(a.coef + (k2 + N01)), C11 = __ldg(a.coef + (k2 + 2 * N01));
+        const T C1 = __ldg(a.coef + (k2 + 3 * N01)), C0 = __ldg(a.coef + (k2 + 4 * N01));
+        const T Cc = __ldg(a.coef + (k2 + 5 * N01));
         if (PF) {
-          const long long n01 = a.N01;
-          point_rhs<T>(col[p + 5], pf[0][p], pf[1][p],
-                       pf[2][p], pf[3][p],
-                       __ldg(a.coef + k2), __ldg(a.coef + n01 + k2), __ldg(a.coef + 2 * n01 + k2),
-                       __ldg(a.coef + 3 * n01 + k2), __ldg(a.coef + 4 * n01 + k2), __ldg(a.coef + 5 * n01 + k2), s0,
-                       s1, s00, s11, s22, a.eta, ku, kv, br);
-          store_point<T, STAGE>(a, idx, ku, kv, pf[4][p],
-                                pf[5][p], pf[6][p],
-                                pf[7][p]);
+          point_rhs<T>(col[p + 5], pf[0][p], pf[1][p], pf[2][p], pf[3][p], C22, C00, C11, C1, C0, Cc, s0, s1, s00,
+                       s11, s22, a.eta, ku, kv, br);
+          yu = pf[4][p];
+          yv = pf[5][p];
+          accu = pf[6][p];
+          accv = pf[7][p];
         } else {
-          point_rhs_global<T>(a, idx, k2, col[p + 5], s0, s1, s00, s11, s22, ku, kv, br);
-          const T accu = (STAGE == 1) ? (T)0 : a.acc[idx];
-          const T accv = (STAGE == 1) ? (T)0 : a.acc[Ntot + idx];
-          store_point<T, STAGE>(a, idx, ku, kv, a.y[idx], a.y[Ntot + idx], accu, accv);
+          point_rhs<T>(col[p + 5], __ldg(a.S + (idx + Ntot)), __ldg(a.aux + (idx + ADD_TIMES_AUUGF * Ntot)),
+                       __ldg(a.aux + (idx + PSI_BACKGROUNDGF * Ntot)), __ldg(a.aux + (idx + WAVESPEEDGF * Ntot)), C22,
+                       C00, C11, C1, C0, Cc, s0, s1, s00, s11, s22, a.eta, ku, kv, br);
+          accu = (STAGE == 1) ? (T)0 : a.acc[idx];
+          accv = (STAGE == 1) ? (T)0 : a.acc[idx + Ntot];
+          yu = a.y[idx];
+          yv = a.y[idx + Ntot];
         }
+        // RK combination and stores (store_point's arithmetic, 32-bit offsets)
+        T ou, ov;
+        rk_combine<T, STAGE>(ku, yu, accu, ou, a.dt);
+        rk_combine<T, STAGE>(kv, yv, accv, ov, a.dt);
+        if (STAGE != 4) {
+          a.acc[idx] = accu;
+          a.acc[idx + Ntot] = accv;
+        }
+        a.out[idx] = ou;
+        a.out[idx + Ntot] = ov;
         if (RESID) {
           const double bb = (double)br;
           r2 += bb * bb * __ldg(a.w + k2);
@@ -321,8 +359,8 @@ static const TileShape kTiles[] = {{4, 1, 0, 0}, {4, 2, 0, 0}, {2, 4, 0, 0}, {8,
                                    {4, 4, 0, 0}, {4, 1, 2, 0}, {4, 2, 2, 0}, {2, 4, 2, 0}, {4, 4, 2, 0},
                                    {8, 2, 2, 0}, {4, 4, 3, 0}, {4, 4, 3, 1}, {8, 2, 3, 2}, {2, 8, 3, 3},
                                    {4, 2, 3, 4}, {4, 2, 4, 0}, {4, 4, 4, 0}, {8, 2, 4, 0}, {2, 4, 4, 0},
-                                   {8, 1, 4, 0}, {4, 1, 4, 0}, {8, 4, 4, 0}, {8, 8, 5, 0}, {8, 8, 5, 1},
-                                   {8, 4, 5, 2}, {8, 16, 5, 3}, {4, 8, 5, 4}, {4, 4, 5, 5}, {8, 4, 5, 6}};
+                                   {8, 1, 4, 0}, {4, 1, 4, 0}, {8, 4, 4, 0}, {8, 8, 5, 0}, {16, 8, 5, 1},
+                                   {8, 4, 5, 2}, {8, 8, 5, 3}, {8, 4, 5, 4}, {8, 16, 5, 5}, {8, 4, 5, 6}};
 constexpr int kNumTiles = sizeof(kTiles) / sizeof(kTiles[0]);
 
 int substep_num_tiles() { return kNumTiles; }
@@ -338,8 +376,15 @@ int substep_interior_blocks(const Dims& d, int tile) {
   return ((d.Nxx0 + 31) / 32) * ((d.Nxx1 + s.by - 1) / s.by) * ((d.Nxx2 + s.p - 1) / s.p);
 }
 
+template <typename T, int STAGE, bool RESID, int BY, int P>
+static void launch_planes(const SubstepArgs& a);
+
 template <typename T, int STAGE, bool RESID, int BY, int P, bool PF>
 static void launch_direct(const SubstepArgs& a) {
+  if (!march_fits(a.d)) {  // 64-bit offsets: the planes kernel
+    launch_planes<T, STAGE, RESID, 8, 1>(a);
+    return;
+  }
   SubDev<T> f = make_dev<T>(a, BY, P);
   constexpr int NT = 32 * BY;
   constexpr int CB = NT / kColThreadsPerColumn;
@@ -464,7 +509,9 @@ static void launch_tile(const SubstepArgs& a) {
     case 26:
     case 27:
     case 28:
-    case 29: launch_march<T>(STAGE, RESID, kTiles[a.tile].v, a); break;
+    case 29:
+      if (!launch_march<T>(STAGE, RESID, kTiles[a.tile].v, a)) launch_planes<T, STAGE, RESID, 8, 1>(a);
+      break;
     default: NRPYELL_FAIL("launch_substep: tile index out of range"); break;
   }
 }
@@ -496,6 +543,10 @@ bool batch_launch_dev(const SubstepArgs& a, SubDev<T>* out) {
     NRPYELL_FAIL("batched substep: the tile must be a shared-memory planes or marching shape");
     return false;
   }
+  if (kTiles[t].kind == 5 && !march_fits(a.d)) {
+    NRPYELL_FAIL("batched substep: a grid is too large for the marching shapes (3 Ntot >= 2^32)");
+    return false;
+  }
   *out = make_dev<T>(a, kTiles[t].by, kTiles[t].p);
   out->n_col_blocks = ((a.d.Nxx1 + kRows - 1) / kRows) * a.d.Nxx2;
   return true;
@@ -524,7 +575,7 @@ static void launch_batch_stage(int tile, const SubDev<T>* devs, const int* offs,
 template <typename T>
 void launch_substep_batch(int stage, bool resid, int tile, const SubDev<T>* devs, const int* offs, int n,
                           int blocks) {
-  if (kTiles[tile].kind == 5) {
+  if (kTiles[tile].kind == 5) {  // batch_launch_dev checked march_fits for every grid
     launch_march_batch<T>(stage, resid, kTiles[tile].v, devs, offs, n, blocks);
     return;
   }

@@ -74,10 +74,19 @@ __device__ __forceinline__ void march_block(const SubDev<T>& a, const int bid, d
   const int b = bid - a.n_col_blocks;
   const int t0 = b % a.tiles0, t1 = (b / a.tiles0) % a.tiles1, t2 = b / (a.tiles0 * a.tiles1);
   const int i00 = t0 * 32 + NGHOSTS, i10 = t1 * BY + NGHOSTS, z0 = t2 * PZ + NGHOSTS;
-  const int N0 = a.N0, top = NGHOSTS + a.Nxx1;
-  const int nz = min(PZ, NGHOSTS + a.Nxx2 - z0);
-  const long long N01 = a.N01, Ntot = a.Ntot;
+  const int N0 = a.N0, top = NGHOSTS + a.Nxx1, Nxx2 = a.Nxx2;
+  const int nz = min(PZ, NGHOSTS + Nxx2 - z0);
+  // element offsets fit in 32 bits (march_fits), so every address is one
+  // 32-bit offset scaled onto a base pointer
+  const unsigned N01 = (unsigned)a.N01, Ntot = (unsigned)a.Ntot;
   const T* __restrict__ u = a.S;
+  // every i2 index below is at most one period outside the interior when
+  // Nxx2 >= 10: one conditional add or subtract instead of a loop
+  const bool once = Nxx2 >= 2 * NGHOSTS;
+  auto wrapz = [&](int j) -> int {
+    if (once) return j < NGHOSTS ? j + Nxx2 : (j >= NGHOSTS + Nxx2 ? j - Nxx2 : j);
+    return wrapm(j, Nxx2);
+  };
   // tiles whose widened planes reach an inner ghost zone gather each point
   // from its source; the others copy rows (16-byte pieces for FP64 when the
   // rows are 16-byte aligned: N0 even and an aligned array)
@@ -85,7 +94,21 @@ __device__ __forceinline__ void march_block(const SubDev<T>& a, const int bid, d
   const bool vec = sizeof(T) == 8 && !inner && (N0 & 1) == 0 && (reinterpret_cast<size_t>(u) & 15) == 0;
   const int i0 = i00 + tx, i1 = i10 + ty;
   const bool valid = i0 < NGHOSTS + a.Nxx0 && i1 < top;
-  const int k2 = i0 + N0 * i1;
+  const unsigned k2 = (unsigned)(i0 + N0 * i1);
+  // the 16-byte pieces of a widened plane this thread copies: offsets within
+  // the plane (global, without the plane term) and in the slot; the same for
+  // every plane
+  constexpr int NV = (NR * HALF + NT - 1) / NT;
+  unsigned vg[NV];
+  int vs[NV];
+#pragma unroll
+  for (int v = 0; v < NV; v++) {
+    const int e = tid + v * NT;
+    const int r = e / HALF, c = 2 * (e - r * HALF);
+    const bool ok = e < NR * HALF && i00 - NGHOSTS + c < N0;
+    vg[v] = (unsigned)(i00 - NGHOSTS + c + N0 * (i10 - NGHOSTS + r));
+    vs[v] = ok ? r * RWS + c : -1;
+  }
 
   // copies of plane p into ring slot p % D (one commit group per plane, empty
   // past the block's last plane)
@@ -94,19 +117,19 @@ __device__ __forceinline__ void march_block(const SubDev<T>& a, const int bid, d
       T* su = ring + (p % D) * L::slot;
       T* pf = su + L::plane;
       const int i2 = z0 + p;
+      const unsigned pl = N01 * (unsigned)i2;
       if (vec) {
-        const T* src = u + (i00 - NGHOSTS) + (long long)N0 * (i10 - NGHOSTS) + N01 * i2;
-        for (int e = tid; e < NR * HALF; e += NT) {
-          const int r = e / HALF, c = 2 * (e - r * HALF);
-          if (i00 - NGHOSTS + c < N0) cp_async<16>(su + r * RWS + c, src + (long long)N0 * r + c);
-        }
+#pragma unroll
+        for (int v = 0; v < NV; v++)
+          if (vs[v] >= 0) cp_async<16>(su + vs[v], u + (vg[v] + pl));
       } else {
+        const unsigned plh = N01 * (unsigned)wrap2(i2 + a.half2, Nxx2);
         for (int e = tid; e < NR * RWS; e += NT) {
           const int r = e / RWS, x = e - r * RWS;
-          int j0 = i00 - NGHOSTS + x, j1 = i10 - NGHOSTS + r, j2 = i2;
+          int j0 = i00 - NGHOSTS + x, j1 = i10 - NGHOSTS + r;
           if (j0 >= N0 || j1 >= top + NGHOSTS) continue;  // never read
+          bool flip = false;
           if (inner) {
-            bool flip = false;
             if (j1 < NGHOSTS) {
               j1 = 2 * NGHOSTS - 1 - j1;
               flip = true;
@@ -118,23 +141,22 @@ __device__ __forceinline__ void march_block(const SubDev<T>& a, const int bid, d
               j0 = 2 * NGHOSTS - 1 - j0;
               flip = !flip;
             }
-            if (flip) j2 = wrap2(i2 + a.half2, a.Nxx2);
           }
-          cp_async<(int)sizeof(T)>(su + r * RWS + x, u + j0 + (long long)N0 * j1 + N01 * j2);
+          cp_async<(int)sizeof(T)>(su + r * RWS + x, u + ((unsigned)(j0 + N0 * j1) + (flip ? plh : pl)));
         }
       }
       if (valid) {
-        const long long idx = k2 + N01 * i2;
-        cp_async<(int)sizeof(T)>(pf + 0 * NT + tid, a.S + Ntot + idx);
-        cp_async<(int)sizeof(T)>(pf + 1 * NT + tid, a.aux + ADD_TIMES_AUUGF * Ntot + idx);
-        cp_async<(int)sizeof(T)>(pf + 2 * NT + tid, a.aux + PSI_BACKGROUNDGF * Ntot + idx);
-        cp_async<(int)sizeof(T)>(pf + 3 * NT + tid, a.aux + WAVESPEEDGF * Ntot + idx);
+        const unsigned idx = k2 + pl;
+        cp_async<(int)sizeof(T)>(pf + 0 * NT + tid, a.S + (idx + Ntot));
+        cp_async<(int)sizeof(T)>(pf + 1 * NT + tid, a.aux + (idx + ADD_TIMES_AUUGF * Ntot));
+        cp_async<(int)sizeof(T)>(pf + 2 * NT + tid, a.aux + (idx + PSI_BACKGROUNDGF * Ntot));
+        cp_async<(int)sizeof(T)>(pf + 3 * NT + tid, a.aux + (idx + WAVESPEEDGF * Ntot));
         cp_async<(int)sizeof(T)>(pf + 4 * NT + tid, a.y + idx);
-        cp_async<(int)sizeof(T)>(pf + 5 * NT + tid, a.y + Ntot + idx);
-        cp_async<(int)sizeof(T)>(pf + 6 * NT + tid, u + k2 + N01 * wrapm(i2 + NGHOSTS, a.Nxx2));
+        cp_async<(int)sizeof(T)>(pf + 5 * NT + tid, a.y + (idx + Ntot));
+        cp_async<(int)sizeof(T)>(pf + 6 * NT + tid, u + (k2 + N01 * (unsigned)wrapz(i2 + NGHOSTS)));
         if (STAGE != 1) {
           cp_async<(int)sizeof(T)>(pf + 7 * NT + tid, a.acc + idx);
-          cp_async<(int)sizeof(T)>(pf + 8 * NT + tid, a.acc + Ntot + idx);
+          cp_async<(int)sizeof(T)>(pf + 8 * NT + tid, a.acc + (idx + Ntot));
         }
       }
     }
@@ -149,13 +171,13 @@ __device__ __forceinline__ void march_block(const SubDev<T>& a, const int bid, d
   double wl2 = 0.0;
   if (valid) {
 #pragma unroll
-    for (int j = 0; j < 10; j++) q[j] = __ldg(u + k2 + N01 * wrapm(z0 - NGHOSTS + j, a.Nxx2));
+    for (int j = 0; j < 10; j++) q[j] = __ldg(u + (k2 + N01 * (unsigned)wrapz(z0 - NGHOSTS + j)));
     C22 = __ldg(a.coef + k2);
-    C00 = __ldg(a.coef + N01 + k2);
-    C11 = __ldg(a.coef + 2 * N01 + k2);
-    C1 = __ldg(a.coef + 3 * N01 + k2);
-    C0 = __ldg(a.coef + 4 * N01 + k2);
-    Cc = __ldg(a.coef + 5 * N01 + k2);
+    C00 = __ldg(a.coef + (k2 + N01));
+    C11 = __ldg(a.coef + (k2 + 2 * N01));
+    C1 = __ldg(a.coef + (k2 + 3 * N01));
+    C0 = __ldg(a.coef + (k2 + 4 * N01));
+    Cc = __ldg(a.coef + (k2 + 5 * N01));
     if (RESID) wl2 = __ldg(a.w + k2);
   }
   double r2 = 0.0;
@@ -183,12 +205,21 @@ __device__ __forceinline__ void march_block(const SubDev<T>& a, const int bid, d
 #pragma unroll
       for (int k = 1; k <= 5; k++) s22 = fma(W<T>::e(k), q[p + 5 + k] + q[p + 5 - k], s22);
       T ku, kv, br;
-      constexpr int FS = NT;
-      point_rhs<T>(q[p + 5], pf[0], pf[FS], pf[2 * FS], pf[3 * FS], C22, C00, C11, C1, C0, Cc, s0, s1, s00, s11, s22,
+      point_rhs<T>(q[p + 5], pf[0], pf[NT], pf[2 * NT], pf[3 * NT], C22, C00, C11, C1, C0, Cc, s0, s1, s00, s11, s22,
                    a.eta, ku, kv, br);
-      const T accu = (STAGE == 1) ? (T)0 : pf[7 * FS];
-      const T accv = (STAGE == 1) ? (T)0 : pf[8 * FS];
-      store_point<T, STAGE>(a, k2 + N01 * (z0 + p), ku, kv, pf[4 * FS], pf[5 * FS], accu, accv);
+      // RK combination and stores (store_point's arithmetic, 32-bit offsets)
+      T accu = (STAGE == 1) ? (T)0 : pf[7 * NT];
+      T accv = (STAGE == 1) ? (T)0 : pf[8 * NT];
+      T ou, ov;
+      rk_combine<T, STAGE>(ku, pf[4 * NT], accu, ou, a.dt);
+      rk_combine<T, STAGE>(kv, pf[5 * NT], accv, ov, a.dt);
+      const unsigned o = k2 + N01 * (unsigned)(z0 + p);
+      if (STAGE != 4) {
+        a.acc[o] = accu;
+        a.acc[o + Ntot] = accv;
+      }
+      a.out[o] = ou;
+      a.out[o + Ntot] = ov;
       if (RESID) {
         const double bb = (double)br;
         r2 += bb * bb * wl2;
@@ -266,7 +297,7 @@ void launch_march_shape(const SubstepArgs& a) {
 // The compiled shapes, by index: (BY, PZ, ring slots D, minimum resident
 // blocks per SM for the register budget).
 #define NRPYELL_MARCH_SHAPES(X)                                                                           \
-  X(0, 8, 8, 3, 2) X(1, 8, 8, 2, 4) X(2, 8, 4, 2, 4) X(3, 8, 16, 2, 4) X(4, 4, 8, 2, 8) X(5, 4, 4, 2, 8) \
+  X(0, 8, 8, 3, 2) X(1, 16, 8, 3, 1) X(2, 8, 4, 2, 4) X(3, 8, 8, 4, 2) X(4, 8, 4, 4, 2) X(5, 8, 16, 3, 2) \
       X(6, 8, 4, 3, 2)
 
 template <typename T, int STAGE, bool RESID>
@@ -313,8 +344,11 @@ void opt_in_shape() {
 
 }  // namespace
 
+bool march_fits(const Dims& d) { return 3.0 * (double)d.Ntot < 4294967296.0; }
+
 template <typename T>
-void launch_march(int stage, bool resid, int v, const SubstepArgs& a) {
+bool launch_march(int stage, bool resid, int v, const SubstepArgs& a) {
+  if (!march_fits(a.d)) return false;
   bool ok = false;
   switch (stage) {
     case 1: ok = resid ? march_stage<T, 1, true>(v, a) : march_stage<T, 1, false>(v, a); break;
@@ -323,9 +357,10 @@ void launch_march(int stage, bool resid, int v, const SubstepArgs& a) {
     default: ok = march_stage<T, 4, false>(v, a); break;
   }
   if (!ok) NRPYELL_FAIL("launch_march: no kernel for this shape");
+  return true;
 }
-template void launch_march<double>(int, bool, int, const SubstepArgs&);
-template void launch_march<float>(int, bool, int, const SubstepArgs&);
+template bool launch_march<double>(int, bool, int, const SubstepArgs&);
+template bool launch_march<float>(int, bool, int, const SubstepArgs&);
 
 template <typename T>
 void prepare_march(int v) {
