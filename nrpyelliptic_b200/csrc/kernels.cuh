@@ -97,6 +97,9 @@ bool launch_march(int stage, bool resid, int v, const SubstepArgs& a);
 // Shared-memory opt-in of a shape's kernels (before a stream capture).
 template <typename T>
 void prepare_march(int v);
+// Interior blocks of shape v's launch on this grid (its split of the planes).
+template <typename T>
+int march_interior_blocks(int v, const SubstepArgs& a);
 
 // ---- bulk-copy pipeline variant (kernels_bulk.cu), FP64 ----
 // Usable when the row length N0 is even and every array is 16-byte aligned.

@@ -373,6 +373,9 @@ int substep_tile_kind(int tile) { return kTiles[tile].kind; }
 
 int substep_interior_blocks(const Dims& d, int tile) {
   const TileShape s = kTiles[tile];
+  // marching shapes: at most one block per (column tile, plane) whatever the
+  // split of the planes into chunks
+  if (s.kind == 5) return ((d.Nxx0 + 31) / 32) * ((d.Nxx1 + s.by - 1) / s.by) * d.Nxx2;
   return ((d.Nxx0 + 31) / 32) * ((d.Nxx1 + s.by - 1) / s.by) * ((d.Nxx2 + s.p - 1) / s.p);
 }
 
@@ -448,11 +451,23 @@ __global__ void __launch_bounds__(256) k_finalize_l2(SubDev<T> a) {
 template <typename T>
 void launch_finalize_forked(const SubstepArgs& a1) {
   prepare_columns();
-  // the tile grid of the stage-1 launch: kind 3 runs the direct 32x4x2 shape
-  // where the bulk pipeline is unavailable
+  // the tile grid of the stage-1 launch, as launch_tile chose it: kind 3 runs
+  // the direct 32x4x2 shape where the bulk pipeline is unavailable, and the
+  // 32-bit-offset kernels (direct, marching) the planes 32x8x1 shape on grids
+  // too large for them
   const TileShape s = kTiles[a1.tile];
-  const bool direct42 = s.kind == 3 && !bulk_available(a1, sizeof(T));
-  SubDev<T> f = make_dev<T>(a1, direct42 ? 4 : s.by, direct42 ? 2 : s.p);
+  const bool fits = march_fits(a1.d);
+  int by = s.by, p = s.p;
+  if (s.kind == 3 && !bulk_available(a1, sizeof(T))) {
+    by = 4;
+    p = 2;
+  }
+  if (!fits && s.kind != 4 && !(s.kind == 3 && bulk_available(a1, sizeof(T)))) {
+    by = 8;
+    p = 1;
+  }
+  SubDev<T> f = make_dev<T>(a1, by, p);
+  if (s.kind == 5 && fits) f.n_tiles = march_interior_blocks<T>(s.v, a1);
   cudaStream_t side = side_stream();
   NRPYELL_CUDA(cudaEventRecord(g_fin_fork, stream()));
   NRPYELL_CUDA(cudaStreamWaitEvent(side, g_fin_fork, 0));

@@ -20,6 +20,12 @@
 // kernel, and the pointwise inputs arrive without a register cost.
 // Column blocks (the radiation BC of the x0max face) come first in the
 // launch, as in the planes kernel.
+#include <functional>
+#include <map>
+#include <queue>
+#include <tuple>
+#include <vector>
+
 #include "substep.cuh"
 
 namespace nrpyell {
@@ -71,11 +77,18 @@ __device__ __forceinline__ void march_block(const SubDev<T>& a, const int bid, d
   }
   T* const ring = reinterpret_cast<T*>(dsm);
   const int tid = threadIdx.x, tx = tid & 31, ty = tid >> 5;
+  // block b: chunk b / C of column tile b % C, the PZ-plane chunks first,
+  // then the msmall-plane chunks (short blocks last, so the last wave is short)
   const int b = bid - a.n_col_blocks;
-  const int t0 = b % a.tiles0, t1 = (b / a.tiles0) % a.tiles1, t2 = b / (a.tiles0 * a.tiles1);
-  const int i00 = t0 * 32 + NGHOSTS, i10 = t1 * BY + NGHOSTS, z0 = t2 * PZ + NGHOSTS;
+  const int C = a.tiles0 * a.tiles1, nbig = C * a.mbig;
+  const int s = b - nbig;
+  const int col = b < nbig ? b % C : s % C;
+  const int z0 = NGHOSTS + (b < nbig ? (b / C) * PZ : a.mbig * PZ + (s / C) * a.msmall);
+  const int zc = b < nbig ? PZ : a.msmall;
+  const int t0 = col % a.tiles0, t1 = col / a.tiles0;
+  const int i00 = t0 * 32 + NGHOSTS, i10 = t1 * BY + NGHOSTS;
   const int N0 = a.N0, top = NGHOSTS + a.Nxx1, Nxx2 = a.Nxx2;
-  const int nz = min(PZ, NGHOSTS + Nxx2 - z0);
+  const int nz = min(zc, NGHOSTS + Nxx2 - z0);
   // element offsets fit in 32 bits (march_fits), so every address is one
   // 32-bit offset scaled onto a base pointer
   const unsigned N01 = (unsigned)a.N01, Ntot = (unsigned)a.Ntot;
@@ -285,11 +298,87 @@ bool march_opt_in() {
   return status_ok();
 }
 
+// Split of each column tile's Nz planes into nb chunks of PZ planes and ns
+// chunks of `small` planes.  The block scheduler hands out blocks in index
+// order as slots free up; with equal chunks the last wave is a partial one
+// (1024 chunks on 296 slots leave SMs idle for ~14 % of a 256x256x32 launch).
+// Greedy list scheduling of the launch's blocks -- column blocks (cost 0.3),
+// then the long chunks, then the short ones (cost planes / PZ + 0.15 for the
+// start-up) -- on `slots` resident blocks picks the split with the shortest
+// makespan.
+struct MarchSplit {
+  int nb, small, ns;
+};
+
+MarchSplit choose_split(int C, int Nz, int PZ, int slots, int ncol) {
+  auto makespan = [&](int nb, int small, int ns) {
+    std::priority_queue<double, std::vector<double>, std::greater<double>> q;
+    for (int i = 0; i < slots; i++) q.push(0.0);
+    auto take = [&](double d, long long n) {
+      for (long long i = 0; i < n; i++) {
+        const double t = q.top();
+        q.pop();
+        q.push(t + d);
+      }
+    };
+    take(0.3, ncol);
+    take(1.15, (long long)C * nb);
+    if (ns > 0) take((double)small / PZ + 0.15, (long long)C * ns);
+    double end = 0.0;
+    while (!q.empty()) {
+      end = q.top();
+      q.pop();
+    }
+    return end;
+  };
+  const int nfull = (Nz + PZ - 1) / PZ;
+  MarchSplit best = {nfull, 0, 0};
+  if (slots <= 0) return best;
+  double tbest = makespan(nfull, 0, 0);
+  for (int nb = 0; nb < nfull; nb++) {
+    const int rest = Nz - nb * PZ;
+    for (int small : {PZ / 2, PZ / 4}) {
+      if (small < 1) continue;
+      const int ns = (rest + small - 1) / small;
+      const double t = makespan(nb, small, ns);
+      if (t < tbest * 0.99) {  // only for a clear gain
+        tbest = t;
+        best = {nb, small, ns};
+      }
+    }
+  }
+  return best;
+}
+
+template <typename T, int STAGE, bool RESID, int BY, int PZ, int D, int MINB>
+MarchSplit march_split(const Dims& d, int ncol) {
+  static std::map<std::tuple<int, int, int, int>, MarchSplit> cache;
+  march_opt_in<T, STAGE, RESID, BY, PZ, D, MINB>();  // the occupancy query needs the shared-memory opt-in
+  int dev = 0;
+  NRPYELL_CUDA(cudaGetDevice(&dev));
+  const auto key = std::make_tuple(dev, d.Nxx0, d.Nxx1, d.Nxx2);
+  auto it = cache.find(key);
+  if (it != cache.end()) return it->second;
+  int per_sm = 0, sms = 0;
+  NRPYELL_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_substep_march<T, STAGE, RESID, BY, PZ, D, MINB>,
+                                                             32 * BY, MarchSmem<T, BY, STAGE, D>::bytes));
+  NRPYELL_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+  const int C = ((d.Nxx0 + 31) / 32) * ((d.Nxx1 + BY - 1) / BY);
+  const MarchSplit s = choose_split(C, d.Nxx2, PZ, per_sm * sms, ncol);
+  cache[key] = s;
+  return s;
+}
+
 template <typename T, int STAGE, bool RESID, int BY, int PZ, int D, int MINB>
 void launch_march_shape(const SubstepArgs& a) {
   if (!march_opt_in<T, STAGE, RESID, BY, PZ, D, MINB>()) return;
   SubDev<T> f = make_dev<T>(a, BY, PZ);
   f.n_col_blocks = ((a.d.Nxx1 + kRows - 1) / kRows) * a.d.Nxx2;
+  // the split is chosen once per grid size and shape (stage 2's occupancy)
+  const MarchSplit sp = march_split<T, 2, false, BY, PZ, D, MINB>(a.d, f.n_col_blocks);
+  f.mbig = sp.nb;
+  f.msmall = sp.small;
+  f.n_tiles = f.tiles0 * f.tiles1 * (sp.nb + sp.ns);
   NRPYELL_LAUNCH_PDL((k_substep_march<T, STAGE, RESID, BY, PZ, D, MINB>), f.n_tiles + f.n_col_blocks, 32 * BY,
                      (MarchSmem<T, BY, STAGE, D>::bytes), f);
 }
@@ -361,6 +450,23 @@ bool launch_march(int stage, bool resid, int v, const SubstepArgs& a) {
 }
 template bool launch_march<double>(int, bool, int, const SubstepArgs&);
 template bool launch_march<float>(int, bool, int, const SubstepArgs&);
+
+template <typename T>
+int march_interior_blocks(int v, const SubstepArgs& a) {
+  const int ncol = ((a.d.Nxx1 + kRows - 1) / kRows) * a.d.Nxx2;
+  switch (v) {
+#define NRPYELL_MARCH(I, BY, PZ, D, MINB)                                               \
+  case I: {                                                                             \
+    const MarchSplit sp = march_split<T, 2, false, BY, PZ, D, MINB>(a.d, ncol);         \
+    return ((a.d.Nxx0 + 31) / 32) * ((a.d.Nxx1 + BY - 1) / BY) * (sp.nb + sp.ns);       \
+  }
+    NRPYELL_MARCH_SHAPES(NRPYELL_MARCH)
+#undef NRPYELL_MARCH
+  }
+  return 0;
+}
+template int march_interior_blocks<double>(int, const SubstepArgs&);
+template int march_interior_blocks<float>(int, const SubstepArgs&);
 
 template <typename T>
 void prepare_march(int v) {

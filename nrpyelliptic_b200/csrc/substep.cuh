@@ -19,6 +19,9 @@ struct SubDev {
   int N0, N1, Nxx0, Nxx1, Nxx2, half2;
   long long N01, Ntot;
   int tiles0, tiles1, tiles2;  // interior tile grid
+  // marching kernel: each (i0,i1) column tile's planes are mbig chunks of PZ
+  // planes (blocks first) and then chunks of msmall planes (blocks last)
+  int mbig, msmall;
   int n_tiles, n_col_blocks, ncol;
   const T* __restrict__ S;     // stage input
   const T* y;                  // y_n (aliases out at stage 4)
@@ -537,6 +540,8 @@ inline SubDev<T> make_dev(const SubstepArgs& a, int by, int p) {
   f.tiles1 = (d.Nxx1 + by - 1) / by;
   f.tiles2 = (d.Nxx2 + p - 1) / p;
   f.n_tiles = f.tiles0 * f.tiles1 * f.tiles2;
+  f.mbig = f.tiles2;
+  f.msmall = 0;
   f.ncol = d.Nxx1 * d.Nxx2;
   f.S = (const T*)a.S;
   f.y = (const T*)a.y;
