@@ -359,8 +359,8 @@ static const TileShape kTiles[] = {{4, 1, 0, 0}, {4, 2, 0, 0}, {2, 4, 0, 0}, {8,
                                    {4, 4, 0, 0}, {4, 1, 2, 0}, {4, 2, 2, 0}, {2, 4, 2, 0}, {4, 4, 2, 0},
                                    {8, 2, 2, 0}, {4, 4, 3, 0}, {4, 4, 3, 1}, {8, 2, 3, 2}, {2, 8, 3, 3},
                                    {4, 2, 3, 4}, {4, 2, 4, 0}, {4, 4, 4, 0}, {8, 2, 4, 0}, {2, 4, 4, 0},
-                                   {8, 1, 4, 0}, {4, 1, 4, 0}, {8, 4, 4, 0}, {8, 8, 5, 0}, {16, 8, 5, 1},
-                                   {8, 4, 5, 2}, {8, 8, 5, 3}, {8, 4, 5, 4}, {8, 16, 5, 5}, {8, 4, 5, 6}};
+                                   {8, 1, 4, 0}, {4, 1, 4, 0}, {8, 4, 4, 0}, {8, 8, 5, 0}, {8, 16, 5, 1},
+                                   {8, 4, 5, 2}, {8, 4, 5, 3}, {8, 8, 5, 4}, {8, 32, 5, 5}, {8, 4, 5, 6}};
 constexpr int kNumTiles = sizeof(kTiles) / sizeof(kTiles[0]);
 
 int substep_num_tiles() { return kNumTiles; }

@@ -386,7 +386,7 @@ void launch_march_shape(const SubstepArgs& a) {
 // The compiled shapes, by index: (BY, PZ, ring slots D, minimum resident
 // blocks per SM for the register budget).
 #define NRPYELL_MARCH_SHAPES(X)                                                                           \
-  X(0, 8, 8, 3, 2) X(1, 16, 8, 3, 1) X(2, 8, 4, 2, 4) X(3, 8, 8, 4, 2) X(4, 8, 4, 4, 2) X(5, 8, 16, 3, 2) \
+  X(0, 8, 8, 3, 2) X(1, 8, 16, 2, 3) X(2, 8, 4, 2, 4) X(3, 8, 4, 2, 3) X(4, 8, 8, 2, 3) X(5, 8, 32, 2, 3) \
       X(6, 8, 4, 3, 2)
 
 template <typename T, int STAGE, bool RESID>
