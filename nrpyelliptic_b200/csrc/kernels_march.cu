@@ -18,8 +18,9 @@
 // Per interior point this reads uu from L2 about 2.9-4.6 times (plane halo)
 // plus (PZ+10)/PZ times (queue), against 14-16 times in the one-plane planes
 // kernel, and the pointwise inputs arrive without a register cost.
-// Column blocks (the radiation BC of the x0max face) come first in the
-// launch, as in the planes kernel.
+// The column blocks (the radiation BC of the x0max face, column_rows) come
+// after the interior blocks in a single-grid launch and before them in a
+// batched one.
 #include <functional>
 #include <map>
 #include <queue>
@@ -65,21 +66,24 @@ struct MarchSmem {
   static constexpr size_t bytes = march > sizeof(double) * kRowsSmem ? march : sizeof(double) * kRowsSmem;
 };
 
-// Block `bid` of one grid's marching launch (column blocks first); dsm is
-// the block's dynamic shared memory (MarchSmem::bytes).
-template <typename T, int STAGE, bool RESID, int BY, int PZ, int D>
+// Block `bid` of one grid's marching launch; dsm is the block's dynamic
+// shared memory (MarchSmem::bytes).  The radiation column blocks come after
+// the interior blocks (COLS_LAST: their short, latency-bound blocks fill the
+// last wave's free slots) or before them (the batched launch's per-grid
+// block ranges).
+template <typename T, int STAGE, bool RESID, int BY, int PZ, int D, bool COLS_LAST>
 __device__ __forceinline__ void march_block(const SubDev<T>& a, const int bid, double* dsm, double* sh, bool* lastp) {
   using L = MarchSmem<T, BY, STAGE, D>;
   constexpr int NT = L::NT, NR = L::NR, RWS = L::RWS, HALF = RWS / 2;
-  if (bid < a.n_col_blocks) {
-    column_rows<T, STAGE, NT>(a, bid, dsm);
+  if (COLS_LAST ? bid >= a.n_tiles : bid < a.n_col_blocks) {
+    column_rows<T, STAGE, NT>(a, COLS_LAST ? bid - a.n_tiles : bid, dsm);
     return;
   }
   T* const ring = reinterpret_cast<T*>(dsm);
   const int tid = threadIdx.x, tx = tid & 31, ty = tid >> 5;
   // block b: chunk b / C of column tile b % C, the PZ-plane chunks first,
   // then the msmall-plane chunks (short blocks last, so the last wave is short)
-  const int b = bid - a.n_col_blocks;
+  const int b = COLS_LAST ? bid : bid - a.n_col_blocks;
   const int C = a.tiles0 * a.tiles1, nbig = C * a.mbig;
   const int s = b - nbig;
   const int col = b < nbig ? b % C : s % C;
@@ -250,7 +254,7 @@ __global__ void __launch_bounds__(32 * BY, MINB) k_substep_march(SubDev<T> a) {
   __shared__ bool last;
   pdl_enter();
   if (*a.done) return;
-  march_block<T, STAGE, RESID, BY, PZ, D>(a, blockIdx.x, dsm, sh, &last);
+  march_block<T, STAGE, RESID, BY, PZ, D, true>(a, blockIdx.x, dsm, sh, &last);
 }
 
 // One substep of many grids in one launch: the blocks of grid c are
@@ -274,7 +278,7 @@ __global__ void __launch_bounds__(32 * BY, MINB)
   }
   const SubDev<T>& a = devs[lo];
   if (*a.done) return;
-  march_block<T, STAGE, RESID, BY, PZ, D>(a, bx - __ldg(offs + lo), dsm, sh, &last);
+  march_block<T, STAGE, RESID, BY, PZ, D, false>(a, bx - __ldg(offs + lo), dsm, sh, &last);
 }
 
 // Opts the kernel into more than 48 KB of dynamic shared memory, once per
@@ -302,10 +306,10 @@ bool march_opt_in() {
 // chunks of `small` planes.  The block scheduler hands out blocks in index
 // order as slots free up; with equal chunks the last wave is a partial one
 // (1024 chunks on 296 slots leave SMs idle for ~14 % of a 256x256x32 launch).
-// Greedy list scheduling of the launch's blocks -- column blocks (cost 0.3),
-// then the long chunks, then the short ones (cost planes / PZ + 0.15 for the
-// start-up) -- on `slots` resident blocks picks the split with the shortest
-// makespan.
+// Greedy list scheduling of the launch's blocks -- the long chunks, then the
+// short ones (cost planes / PZ + 0.15 for the start-up), then the column
+// blocks (cost 0.3) -- on `slots` resident blocks picks the split with the
+// shortest makespan.
 struct MarchSplit {
   int nb, small, ns;
 };
@@ -321,9 +325,9 @@ MarchSplit choose_split(int C, int Nz, int PZ, int slots, int ncol) {
         q.push(t + d);
       }
     };
-    take(0.3, ncol);
     take(1.15, (long long)C * nb);
     if (ns > 0) take((double)small / PZ + 0.15, (long long)C * ns);
+    take(0.3, ncol);
     double end = 0.0;
     while (!q.empty()) {
       end = q.top();

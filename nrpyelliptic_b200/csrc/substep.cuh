@@ -401,8 +401,11 @@ __device__ void column_block(const SubDev<T>& a, int cb) {
 constexpr int kRows = 32;
 
 // Shared memory of column_rows, in doubles: F[2][kRows+10][12], drf and fvs
-// [kRows][2][6], kl [kRows][2], kk [kRows][2][5].
-constexpr int kRowsSmem = 2 * (kRows + 10) * 12 + 2 * kRows * 12 + kRows * 2 + kRows * 10;
+// [kRows][2][6], kl [kRows][2], kk [kRows][2][5], and G[kRows][kColG]: per
+// column the values the RHS of its last interior point reads outside F
+// (uu at i2 +- 1..5, vv, the three auxevol fields, the six metric weights).
+constexpr int kColG = 20;
+constexpr int kRowsSmem = 2 * (kRows + 10) * 12 + 2 * kRows * 12 + kRows * 2 + kRows * 10 + kRows * kColG;
 
 template <typename T, int STAGE, int NT>
 __device__ void column_rows(const SubDev<T>& a, int cb, double* smem) {
@@ -413,6 +416,7 @@ __device__ void column_rows(const SubDev<T>& a, int cb, double* smem) {
   double(*fvs)[2][6] = reinterpret_cast<double(*)[2][6]>(smem + 2 * NRW * NQ + kRows * 12);
   double(*kl)[2] = reinterpret_cast<double(*)[2]>(smem + 2 * NRW * NQ + 2 * kRows * 12);
   double(*kk)[2][5] = reinterpret_cast<double(*)[2][5]>(smem + 2 * NRW * NQ + 2 * kRows * 12 + 2 * kRows);
+  double(*G)[kColG] = reinterpret_cast<double(*)[kColG]>(smem + 2 * NRW * NQ + 2 * kRows * 12 + 2 * kRows + 10 * kRows);
   const int tid = threadIdx.x;
   const int nb1 = (a.Nxx1 + kRows - 1) / kRows;
   const int i1a = NGHOSTS + (cb % nb1) * kRows;
@@ -433,6 +437,27 @@ __device__ void column_rows(const SubDev<T>& a, int cb, double* smem) {
       i2s = i2h;
     }
     F[g][j][q] = (double)__ldg(a.S + g * a.Ntot + (N0 - NQ + q) + (long long)N0 * i1 + a.N01 * i2s);
+  }
+  // the rest of each column's last-interior-point inputs, spread over the
+  // block (item m of column c: 0..9 uu at i2 -+ 1..5, 10 vv, 11..13 auxevol,
+  // 14..19 metric weights)
+  for (int e = tid; e < kRows * kColG; e += NT) {
+    const int c = e / kColG, m = e - c * kColG;
+    if (c >= ncol) continue;
+    const long long line = (N0 - NGHOSTS - 1) + (long long)N0 * (i1a + c);
+    const T* src;
+    if (m < 10) {
+      const int k = m / 2 + 1;
+      src = a.S + line + a.N01 * wrap2((m & 1) ? i2 + k : i2 - k, a.Nxx2);
+    } else if (m == 10) {
+      src = a.S + a.Ntot + line + a.N01 * i2;
+    } else if (m < 14) {
+      const int gf = m == 11 ? ADD_TIMES_AUUGF : (m == 12 ? PSI_BACKGROUNDGF : WAVESPEEDGF);
+      src = a.aux + gf * a.Ntot + line + a.N01 * i2;
+    } else {
+      src = a.coef + (m - 14) * a.N01 + line;
+    }
+    G[c][m] = (double)__ldg(src);
   }
   __syncthreads();
   // radial derivatives at the last interior point and the 5 layers (items
@@ -456,7 +481,6 @@ __device__ void column_rows(const SubDev<T>& a, int cb, double* smem) {
     } else {
       const int c = it - kRows * 12;
       if (c >= ncol) continue;
-      const int i1 = i1a + c, i0 = N0 - NGHOSTS - 1;
       const double* row = F[0][c + NGHOSTS];
       T s0 = 0, s1 = 0, s00 = 0, s11 = 0, s22 = 0;
 #pragma unroll
@@ -468,15 +492,12 @@ __device__ void column_rows(const SubDev<T>& a, int cb, double* smem) {
         s00 = fma(W<T>::e(k), ap + am, s00);
         s11 = fma(W<T>::e(k), bp + bm, s11);
       }
-      const T* u = a.S;
-      const long long line = i0 + (long long)N0 * i1;
+      const double* gc = G[c];
 #pragma unroll
-      for (int k = 1; k <= 5; k++)
-        s22 = fma(W<T>::e(k),
-                  __ldg(u + line + a.N01 * wrap2(i2 + k, a.Nxx2)) + __ldg(u + line + a.N01 * wrap2(i2 - k, a.Nxx2)),
-                  s22);
+      for (int k = 1; k <= 5; k++) s22 = fma(W<T>::e(k), (T)gc[2 * k - 1] + (T)gc[2 * k - 2], s22);
       T ku, kv, br;
-      point_rhs_global<T>(a, line + a.N01 * i2, i0 + N0 * i1, (T)row[6], s0, s1, s00, s11, s22, ku, kv, br);
+      point_rhs<T>((T)row[6], (T)gc[10], (T)gc[11], (T)gc[12], (T)gc[13], (T)gc[14], (T)gc[15], (T)gc[16],
+                   (T)gc[17], (T)gc[18], (T)gc[19], s0, s1, s00, s11, s22, a.eta, ku, kv, br);
       kl[c][0] = (double)ku;
       kl[c][1] = (double)kv;
     }
