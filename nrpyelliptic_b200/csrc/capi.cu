@@ -323,6 +323,7 @@ int nrpyell_time_fused(griddata_struct* g, const REAL dt, const int stage, const
   const StateBuffers b = buffers_of(&g->gridfuncs);
   const RelaxParams rp = relax_params(&g->params, dt);
   const int tile = tuned_tile<double>(d, rt, bt, w, sc, b, rp);
+  prepare_substep<double>(tile);
   cudaEvent_t e0, e1;
   NRPYELL_CUDA(cudaEventCreate(&e0));
   NRPYELL_CUDA(cudaEventCreate(&e1));

@@ -483,6 +483,7 @@ template <typename T>
 void prepare_substep(int tile) {
   if (kTiles[tile].kind == 3) prepare_bulk(kTiles[tile].v);
   if (kTiles[tile].kind == 5) prepare_march<T>(kTiles[tile].v);
+  if (kTiles[tile].kind == 3 || kTiles[tile].kind == 5) prepare_columns();  // side stream and events
 }
 template void prepare_substep<double>(int);
 template void prepare_substep<float>(int);
