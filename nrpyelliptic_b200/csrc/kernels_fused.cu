@@ -36,11 +36,18 @@ template <typename T, int STAGE, bool RESID, int BY, int P, bool PF>
 __global__ void __launch_bounds__(32 * BY) k_substep(SubDev<T> a) {
   constexpr int NT = 32 * BY;
   __shared__ double sh[NT / 32 > 8 ? NT / 32 : 8];
+  // radiation columns: blocks of 256 threads take 32 columns by rows
+  // (column_rows), narrower blocks 16 threads per column (column_block)
+  constexpr bool ROWS = NT >= 256;
+  __shared__ double csm[ROWS ? kRowsSmem : 1];
   __shared__ bool last;
   pdl_enter();
   if (*a.done) return;
   if ((int)blockIdx.x < a.n_col_blocks) {
-    column_block<T, STAGE, NT>(a, blockIdx.x);
+    if constexpr (ROWS)
+      column_rows<T, STAGE, NT>(a, blockIdx.x, csm);
+    else
+      column_block<T, STAGE, NT>(a, blockIdx.x);
     return;
   }
   const int tid = threadIdx.x;
@@ -391,7 +398,7 @@ static void launch_direct(const SubstepArgs& a) {
   SubDev<T> f = make_dev<T>(a, BY, P);
   constexpr int NT = 32 * BY;
   constexpr int CB = NT / kColThreadsPerColumn;
-  f.n_col_blocks = (f.ncol + CB - 1) / CB;
+  f.n_col_blocks = NT >= 256 ? ((a.d.Nxx1 + kRows - 1) / kRows) * a.d.Nxx2 : (f.ncol + CB - 1) / CB;
   NRPYELL_LAUNCH_PDL((k_substep<T, STAGE, RESID, BY, P, PF>), f.n_tiles + f.n_col_blocks, NT, 0, f);
 }
 
