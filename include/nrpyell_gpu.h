@@ -202,7 +202,7 @@ int nrpyell_relax(griddata_struct *griddata, const REAL dt, const REAL log10_tol
  * accumulated in FP64) from the initial y_n until log10 L2 <= log10_switch or
  * the residual stalls -- its best value so far has not dropped below
  * stall_factor (e.g. 0.98) times itself for stall_window steps; the
- * relaxation residual oscillates, so only the running minimum is judged, and
+ * relaxation residual oscillates, so only the running minimum counts, and
  * only once it is within two decades of log10_switch --
  * then FP64 from that state to
  * log10_tol.  steps_fp32 / steps_fp64 receive the RK4 steps of each phase;

@@ -3,7 +3,7 @@ parameters to the coefficients of a POD basis of uu built from solutions the
 relaxation itself generates; vv is guessed as eta * uu (the steady state of
 uu_rhs = vv - eta uu).  The guess is used only when its residual L2 is below
 the zero guess's (else the zero guess is the fallback), and the FP64
-relaxation from either start is the judge of the final error.
+relaxation from either start decides the final error.
 
     python -m nrpyelliptic_b200.learned [--train 4096] [--test 256] [--modes 256] [--epochs 400]
 
