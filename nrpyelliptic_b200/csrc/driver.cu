@@ -134,13 +134,20 @@ int tuned_tile(const Dims& d, RfmTables* rt, BcTables* bt, FusedWork* w, Scratch
   NRPYELL_CUDA(cudaEventCreate(&e1));
   int best = 0;
   float best_ms = 1e30f;
+  // Each shape is timed on stages 1-3 back to back, as a relaxation runs
+  // them (a shape can be fast at one stage and slow at the next); stage 4
+  // would write y_n, the caller's state, so it is left out -- stages 1-3
+  // write only the running total and the stage buffers.
   for (int t = 0; t < substep_num_tiles(); t++) {
-    const SubstepArgs a = substep_args(d, rt, bt, sc, b, rp, 2, w->zero_flag, w->state, t);
-    launch_substep<T>(2, a);
+    SubstepArgs a[3];
+    for (int st = 1; st <= 3; st++) a[st - 1] = substep_args(d, rt, bt, sc, b, rp, st, w->zero_flag, w->state, t);
+    prepare_substep<T>(t);
+    for (int st = 1; st <= 3; st++) launch_substep<T>(st, a[st - 1]);
     float tmin = 1e30f;
     for (int rep = 0; rep < 3; rep++) {
       NRPYELL_CUDA(cudaEventRecord(e0, stream()));
-      for (int i = 0; i < 10; i++) launch_substep<T>(2, a);
+      for (int i = 0; i < 4; i++)
+        for (int st = 1; st <= 3; st++) launch_substep<T>(st, a[st - 1]);
       NRPYELL_CUDA(cudaEventRecord(e1, stream()));
       NRPYELL_CUDA(cudaEventSynchronize(e1));
       float ms = 0.0f;
