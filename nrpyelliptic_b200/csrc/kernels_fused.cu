@@ -71,6 +71,9 @@ __global__ void __launch_bounds__(32 * BY) k_substep(SubDev<T> a) {
   if (i0 < NGHOSTS + a.Nxx0 && i1 < top) {
     const T* __restrict__ u = a.S;
     const unsigned k2 = (unsigned)(i0 + N0 * i1);
+    // at stage 1 the stage input is y_n itself: y_n's uu and vv at a point
+    // are its col[] value and its vv
+    const bool y_is_s = STAGE == 1 && a.y == a.S;
     // uu along i2 for planes z0-5 .. z0+P+4 (wrapped by 2 pi)
     T col[P + 10];
 #pragma unroll
@@ -86,8 +89,8 @@ __global__ void __launch_bounds__(32 * BY) k_substep(SubDev<T> a) {
         pf[1][p] = __ldg(a.aux + (idx + ADD_TIMES_AUUGF * Ntot));
         pf[2][p] = __ldg(a.aux + (idx + PSI_BACKGROUNDGF * Ntot));
         pf[3][p] = __ldg(a.aux + (idx + WAVESPEEDGF * Ntot));
-        pf[4][p] = a.y[idx];
-        pf[5][p] = a.y[idx + Ntot];
+        pf[4][p] = y_is_s ? col[p + 5] : a.y[idx];
+        pf[5][p] = y_is_s ? pf[0][p] : a.y[idx + Ntot];
         pf[6][p] = (STAGE == 1) ? (T)0 : a.acc[idx];
         pf[7][p] = (STAGE == 1) ? (T)0 : a.acc[idx + Ntot];
       }
@@ -135,8 +138,8 @@ __global__ void __launch_bounds__(32 * BY) k_substep(SubDev<T> a) {
                        C00, C11, C1, C0, Cc, s0, s1, s00, s11, s22, a.eta, ku, kv, br);
           accu = (STAGE == 1) ? (T)0 : a.acc[idx];
           accv = (STAGE == 1) ? (T)0 : a.acc[idx + Ntot];
-          yu = a.y[idx];
-          yv = a.y[idx + Ntot];
+          yu = y_is_s ? col[p + 5] : a.y[idx];
+          yv = y_is_s ? __ldg(a.S + (idx + Ntot)) : a.y[idx + Ntot];
         }
         // RK combination and stores (store_point's arithmetic, 32-bit offsets)
         T ou, ov;

@@ -112,6 +112,9 @@ __device__ __forceinline__ void march_block(const SubDev<T>& a, const int bid, d
   const int i0 = i00 + tx, i1 = i10 + ty;
   const bool valid = i0 < NGHOSTS + a.Nxx0 && i1 < top;
   const unsigned k2 = (unsigned)(i0 + N0 * i1);
+  // at stage 1 the stage input is y_n itself: y_n's uu and vv at the point
+  // are the plane's centre value and the vv already copied
+  const bool y_is_s = STAGE == 1 && a.y == a.S;
   // the 16-byte pieces of a widened plane this thread copies: offsets within
   // the plane (global, without the plane term) and in the slot; the same for
   // every plane
@@ -168,8 +171,10 @@ __device__ __forceinline__ void march_block(const SubDev<T>& a, const int bid, d
         cp_async<(int)sizeof(T)>(pf + 1 * NT + tid, a.aux + (idx + ADD_TIMES_AUUGF * Ntot));
         cp_async<(int)sizeof(T)>(pf + 2 * NT + tid, a.aux + (idx + PSI_BACKGROUNDGF * Ntot));
         cp_async<(int)sizeof(T)>(pf + 3 * NT + tid, a.aux + (idx + WAVESPEEDGF * Ntot));
-        cp_async<(int)sizeof(T)>(pf + 4 * NT + tid, a.y + idx);
-        cp_async<(int)sizeof(T)>(pf + 5 * NT + tid, a.y + (idx + Ntot));
+        if (!y_is_s) {
+          cp_async<(int)sizeof(T)>(pf + 4 * NT + tid, a.y + idx);
+          cp_async<(int)sizeof(T)>(pf + 5 * NT + tid, a.y + (idx + Ntot));
+        }
         cp_async<(int)sizeof(T)>(pf + 6 * NT + tid, u + (k2 + N01 * (unsigned)wrapz(i2 + NGHOSTS)));
         if (STAGE != 1) {
           cp_async<(int)sizeof(T)>(pf + 7 * NT + tid, a.acc + idx);
@@ -228,8 +233,8 @@ __device__ __forceinline__ void march_block(const SubDev<T>& a, const int bid, d
       T accu = (STAGE == 1) ? (T)0 : pf[7 * NT];
       T accv = (STAGE == 1) ? (T)0 : pf[8 * NT];
       T ou, ov;
-      rk_combine<T, STAGE>(ku, pf[4 * NT], accu, ou, a.dt);
-      rk_combine<T, STAGE>(kv, pf[5 * NT], accv, ov, a.dt);
+      rk_combine<T, STAGE>(ku, y_is_s ? q[p + 5] : pf[4 * NT], accu, ou, a.dt);
+      rk_combine<T, STAGE>(kv, y_is_s ? pf[0] : pf[5 * NT], accv, ov, a.dt);
       const unsigned o = k2 + N01 * (unsigned)(z0 + p);
       if (STAGE != 4) {
         a.acc[o] = accu;
