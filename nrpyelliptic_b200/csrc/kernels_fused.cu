@@ -23,8 +23,10 @@
 // This file holds the direct variant: each thread owns an (i0,i1) pair and P
 // consecutive i2 planes, holds uu along i2 in registers and reads the rest of
 // its 31-point star through L1 (optionally loading the pointwise inputs of
-// all P planes before the first store).  kernels_bulk.cu holds the
-// bulk-copy pipeline variant; the autotuner picks among the shapes of both.
+// all P planes before the first store), and the shared-memory planes
+// variant.  kernels_march.cu holds the marching variant and kernels_bulk.cu
+// the bulk-copy pipeline variant; the autotuner picks among the shapes of
+// all of them (the tile table below).
 // The metric factors of the RHS depend on (i0,i1) only and are folded into
 // six per-(i0,i1) weights (tables.cu), leaving one division per point.
 #include "substep.cuh"

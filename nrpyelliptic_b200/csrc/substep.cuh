@@ -1,8 +1,10 @@
 // Device code shared by the fused RK4 substep kernels (kernels_fused.cu: one
-// thread per (i0,i1) column of P points reading through L1; kernels_bulk.cu:
-// tiles staged in shared memory by bulk asynchronous copies): the launch
-// arguments, the point RHS, the RK combination, the radiation-BC column work
-// and the stop-test reduction.  Every variant evaluates a point with the same
+// thread per (i0,i1) column of P points reading through L1, or the block's
+// planes staged in shared memory; kernels_march.cu: blocks marching along i2
+// with the planes copied ahead by cp.async; kernels_bulk.cu: tiles staged in
+// shared memory by bulk asynchronous copies): the launch arguments, the point
+// RHS, the RK combination, the radiation-BC column work and the stop-test
+// reduction.  Every variant evaluates a point with the same
 // operations in the same order, so all of them produce identical bits.
 #pragma once
 

@@ -1,9 +1,10 @@
 """Every tile shape of the fused substep kernel (direct, prefetching, TMA
-pipeline, shared-memory planes) against the reference's golden steps and
-against each other.
+pipeline, shared-memory planes, marching along i2) against the reference's
+golden steps and against each other.
 
 The shapes differ only in how points are assigned to threads and how the
-stencil is fetched (through L1, or staged in shared memory); the arithmetic
+stencil is fetched (through L1, staged in shared memory, or copied ahead by
+asynchronous copies); the arithmetic
 per point is the same, so RK4 steps are bit-identical across shapes.  The L2
 norm of the stop test sums per-tile partials, whose number depends on the
 shape, so relaxation histories agree to rounding and step counts to +-1.
