@@ -16,8 +16,9 @@ ours:      solves on device-resident buffers through nrpyell_relax (value),
            solves per rank (replicas; no data-path collective), barrier and
            max-over-ranks timing.
 reference: the reference's own C (oracle/_ref, built from its sources with
-           OpenMP) timed on the host cores on a bounded sample of main.c loop
-           iterations of the same workload; rank 0 only.
+           OpenMP) on the host cores: every step is one complete solve of the
+           same workload from the zero guess (main.c's loop with the stop
+           test); rank 0 only.
 """
 import argparse
 import ctypes as C
@@ -189,36 +190,94 @@ def cpu_time_per_iteration(cfg, seconds, threads=None):
     return t_done / n_done, kind, cores, n_done
 
 
+def cpu_solver(cfg):
+    """One complete solve of cfg from the zero guess on the host cores per
+    call: the reference's own build (main.c's loop with the stop test,
+    refh_relax) when present, else the oracle port.  Returns (solve,
+    cleanup, kind, cores); solve() returns (seconds, steps, converged)."""
+    from nrpyelliptic_b200 import abi
+    from nrpyelliptic_b200.problem import set_physical_params
+    from oracle import build as obuild
+    ref = obuild.ref_lib_path(cpu_isa())
+    P = C.POINTER
+    if os.path.exists(ref):
+        lib = C.CDLL(ref)
+        lib.refh_setup.restype = C.c_double
+        lib.refh_setup.argtypes = [P(abi.griddata_struct), P(C.c_int), P(abi.paramstruct), C.c_double]
+        lib.refh_relax.restype = C.c_int
+        lib.refh_relax.argtypes = [P(abi.griddata_struct), C.c_double, C.c_double, C.c_int, C.c_double, abi.PREAL,
+                                   P(C.c_int)]
+        lib.refh_free.argtypes = [P(abi.griddata_struct)]
+        lib.refh_max_threads.restype = C.c_int
+        lib.set_Cparameters_to_default.argtypes = [P(abi.paramstruct)]
+        phys = abi.paramstruct()
+        lib.set_Cparameters_to_default(C.byref(phys))
+        set_physical_params(phys, cfg)
+        g = abi.griddata_struct()
+        dt = lib.refh_setup(C.byref(g), (C.c_int * 3)(*cfg.Nxx), C.byref(phys), cfg.CFL)
+        relax = lib.refh_relax
+        kind, cores = "reference", lib.refh_max_threads()
+        cleanup = lambda: lib.refh_free(C.byref(g))
+    else:
+        sys.path.insert(0, os.path.join(ROOT, "tests"))
+        from _util import oracle, problem_grid
+
+        from nrpyelliptic_b200.problem import Problem
+        o = oracle()
+        prob = Problem(cfg)
+        hg = problem_grid(prob)
+        g = hg.griddata()
+        dt = prob.dt
+        relax = o.oracle_relax
+        kind, cores = "port", os.cpu_count()
+        cleanup = lambda: None
+    p = g.params
+    n2 = 2 * p.Nxx_plus_2NGHOSTS0 * p.Nxx_plus_2NGHOSTS1 * p.Nxx_plus_2NGHOSTS2 * 8
+
+    def solve(max_steps=40000):
+        C.memset(g.gridfuncs.y_n_gfs, 0, n2)  # initial_guess_all_points: uu = vv = 0
+        steps = C.c_int(0)
+        t0 = time.perf_counter()
+        rc = relax(C.byref(g), dt, TOL, max_steps, cfg.R_L2, None, C.byref(steps))
+        return time.perf_counter() - t0, steps.value, rc == 0
+
+    return solve, cleanup, kind, cores
+
+
 def run_reference(args, dist):
+    """The reference's own CPU implementation of the path: every bench step is
+    one complete solve of the workload from the zero guess to the tolerance
+    (main.c's loop: residual, L2, RK4 step, with the stop test)."""
     from nrpyelliptic_b200.problem import CONFIGS
     if dist.rank != 0:
         return
     cfg = CONFIGS[args.config]
-    steps_ref = reference_steps(args.config)
-    if steps_ref is None:
-        print(json.dumps({"impl": "reference", "unavailable": "no recorded reference step count for " + args.config}))
-        return
-    per_step = []
-    meta = None
+    solve, cleanup, kind, cores = cpu_solver(cfg)
+    times, steps_seen = [], set()
     for i in range(args.warmup + args.steps):
-        t_it, kind, cores, n = cpu_time_per_iteration(cfg, max(2.0, args.cpu_seconds / 4))
-        meta = (kind, cores, n)
+        t, n, ok = solve(args.max_steps)
+        if not ok:
+            raise RuntimeError("reference solve did not converge in %d steps" % args.max_steps)
+        steps_seen.add(n)
         if i >= args.warmup:
-            per_step.append(t_it)
-    t_it = statistics.mean(per_step)
-    t_solve = t_it * (steps_ref + 1)
+            times.append(t)
+    cleanup()
+    t_solve = sum(times) / len(times)
     value = 1.0 / t_solve
-    kind, cores, n = meta
-    sample = ("%d main.c-loop iterations (residual, L2, RK4 step) of %s per step, x %d iterations to 1e-10 "
-              "(the reference's own converged step count + 1)" % (n, args.config, steps_ref + 1))
+    # per-iteration sample of the same loop, for comparison with the GPU arm's cpu_baseline
+    t_it, _, _, n_it = cpu_time_per_iteration(cfg, max(2.0, args.cpu_seconds / 4))
+    sample = ("%d complete solves of %s from the zero guess to log10 L2 <= %g (main.c loop: residual, L2, "
+              "RK4 step), %s steps each" % (args.steps, args.config, TOL, "/".join(str(s) for s in sorted(steps_seen))))
     line = {"metric": METRIC, "value": value, "unit": "solves/s", "n_gpus": args.gpus, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": t_solve * 1e3, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded puncture parameters, zero guess)",
             "impl": "reference",
             "config": {"workload": args.config, "grid": list(cfg.Nxx), "tolerance_log10": TOL,
-                       "steps_to_tolerance": steps_ref, "parallelism": "host OpenMP"},
+                       "steps_to_tolerance": max(steps_seen), "parallelism": "host OpenMP"},
             "cpu_baseline": {"value": value, "unit": "solves/s", "cores": cores, "kind": kind, "sample": sample},
-            "e2e": {"value": value, "unit": "solves/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+            "e2e": {"value": value, "unit": "solves/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+            "per_iteration_sample": {"s_per_iteration": t_it, "iterations": n_it,
+                                     "solves_per_s_extrapolated": 1.0 / (t_it * (max(steps_seen) + 1))}}
     print(json.dumps(line))
 
 

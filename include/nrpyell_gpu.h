@@ -77,10 +77,17 @@ REAL L2_norm_of_gf(const paramstruct *NRPYELL_RESTRICT params, const int gf_inde
  * memory (no counterpart in the reference): all working memory is one
  * fixed-size array in the library (37.5 KB per GPU, held until exit), so no
  * cudaMalloc/cudaFree is ever called.  Grids are limited to 2048 x 2048
- * points in xx0 x xx1 (ghosts included); larger ones are rejected with an
- * error and NaN.  Calls share the array: calls that overlap on the GPU race.
- * The first call on a device looks the array up (cudaGetSymbolAddress) and
- * should come before any stream capture. */
+ * points in xx0 x xx1 (ghosts included), and Nxx_plus_2NGHOSTSi must equal
+ * Nxxi + 2 NGHOSTS; other grids are rejected with an error and NaN before
+ * any GPU work.  Calls share the array: calls that overlap on the GPU race.
+ * Every call copies xx0/xx1 from pageable host memory and waits for its
+ * result, so it must not be called while the library's stream (or the legacy
+ * default stream) is being captured.  The first call on a device looks the
+ * array up (cudaGetSymbolAddress); with CUDA's lazy module loading (the
+ * default) that first lookup also loads the library's GPU code, which makes
+ * the driver's own allocations for code and globals -- make the first call
+ * at start-up, before a fixed arena or quota is in force, or run with
+ * CUDA_MODULE_LOADING=EAGER for a strict guarantee. */
 REAL L2_norm_of_gf_noalloc(const paramstruct *NRPYELL_RESTRICT params, const int gf_index,
                            const REAL integration_radius, REAL *NRPYELL_RESTRICT xx[3],
                            const REAL *NRPYELL_RESTRICT in_gf);
@@ -103,6 +110,9 @@ void nrpyell_set_exit_on_error(int enable);
 int nrpyell_abi_layout(int *out, int n);
 /* Number of kernel launches issued by this process so far. */
 long long nrpyell_launch_count(void);
+/* Number of device (cudaMalloc) and managed allocations the library has
+ * made so far in this process. */
+long long nrpyell_device_alloc_count(void);
 
 /* How MoL_step_forward_in_time runs.
  *  NRPYELL_STEP_FUSED (default): per RK4 substep one fused RHS + update

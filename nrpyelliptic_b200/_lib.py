@@ -39,6 +39,7 @@ EXPORTS = {
     "nrpyell_set_exit_on_error": (None, [C.c_int]),
     "nrpyell_abi_layout": (C.c_int, [P(C.c_int), C.c_int]),
     "nrpyell_launch_count": (C.c_longlong, []),
+    "nrpyell_device_alloc_count": (C.c_longlong, []),
     "nrpyell_set_step_mode": (None, [C.c_int]),
     "nrpyell_get_step_mode": (C.c_int, []),
     "nrpyell_set_device": (C.c_int, [C.c_int]),

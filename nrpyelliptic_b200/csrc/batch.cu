@@ -52,13 +52,13 @@ bool ensure_batch(int n, int hist_len, int partials_per) {
   g_batch.n = n;
   g_batch.hist_len = hist_len;
   g_batch.partials_per = partials_per;
-  NRPYELL_CUDA(cudaMalloc(&g_batch.state, sizeof(int) * kStateInts * n));
-  NRPYELL_CUDA(cudaMalloc(&g_batch.stall, sizeof(double) * 2 * n));
-  NRPYELL_CUDA(cudaMalloc(&g_batch.history, sizeof(double) * (size_t)hist_len * n));
-  NRPYELL_CUDA(cudaMalloc(&g_batch.partials, sizeof(double) * (size_t)partials_per * n));
-  NRPYELL_CUDA(cudaMalloc(&g_batch.tickets, sizeof(unsigned int) * n));
-  NRPYELL_CUDA(cudaMalloc(&g_batch.offs, sizeof(int) * n));
-  NRPYELL_CUDA(cudaMalloc(&g_batch.devs, sizeof(SubDev<double>) * 5 * n));
+  NRPYELL_CUDA(dev_alloc(&g_batch.state, sizeof(int) * kStateInts * n));
+  NRPYELL_CUDA(dev_alloc(&g_batch.stall, sizeof(double) * 2 * n));
+  NRPYELL_CUDA(dev_alloc(&g_batch.history, sizeof(double) * (size_t)hist_len * n));
+  NRPYELL_CUDA(dev_alloc(&g_batch.partials, sizeof(double) * (size_t)partials_per * n));
+  NRPYELL_CUDA(dev_alloc(&g_batch.tickets, sizeof(unsigned int) * n));
+  NRPYELL_CUDA(dev_alloc(&g_batch.offs, sizeof(int) * n));
+  NRPYELL_CUDA(dev_alloc(&g_batch.devs, sizeof(SubDev<double>) * 5 * n));
   NRPYELL_CUDA(cudaMemset(g_batch.tickets, 0, sizeof(unsigned int) * n));
   return status_ok();
 }

@@ -64,6 +64,8 @@ cudaStream_t side_stream() {
 void count_launch(int n) { g_launches += n; }
 long long launch_count() { return g_launches; }
 void set_launch_count(long long n) { g_launches = n; }
+static long long g_allocs = 0;
+void count_alloc() { g_allocs++; }
 
 bool check_device_pointer(const void* ptr, const char* what) {
   char msg[256];
@@ -211,6 +213,7 @@ void nrpyell_clear_status(void) {
 }
 void nrpyell_set_exit_on_error(int enable) { g_exit_on_error = enable != 0; }
 long long nrpyell_launch_count(void) { return g_launches; }
+long long nrpyell_device_alloc_count(void) { return g_allocs; }
 
 int nrpyell_abi_layout(int* out, int n) {
   const int v[] = {(int)sizeof(paramstruct),
@@ -303,7 +306,7 @@ float nrpyell_event_elapsed_ms(int a, int b) {
 void nrpyell_flush_l2(void) {
   static void* buf = nullptr;
   const size_t bytes = (size_t)256 << 20;
-  if (!buf) NRPYELL_CUDA(cudaMalloc(&buf, bytes));
+  if (!buf) NRPYELL_CUDA(dev_alloc(&buf, bytes));
   NRPYELL_CUDA(cudaMemsetAsync(buf, 0x5a, bytes, stream()));
 }
 
@@ -372,7 +375,7 @@ void nrpyell_release_tables(void) {
 
 void* nrpyell_device_malloc(size_t bytes) {
   void* p = nullptr;
-  NRPYELL_CUDA(cudaMalloc(&p, bytes));
+  NRPYELL_CUDA(dev_alloc(&p, bytes));
   return p;
 }
 void nrpyell_device_free(void* ptr) {
@@ -404,7 +407,7 @@ int nrpyell_memset(void* dst, int value, size_t bytes) {
 void MoL_malloc_y_n_gfs(const paramstruct* params, MoL_gridfunctions_struct* gridfuncs) {
   const size_t n = (size_t)params->Nxx_plus_2NGHOSTS0 * params->Nxx_plus_2NGHOSTS1 * params->Nxx_plus_2NGHOSTS2;
   void* p = nullptr;
-  NRPYELL_CUDA(cudaMallocManaged(&p, sizeof(REAL) * NUM_EVOL_GFS * n));
+  NRPYELL_CUDA(managed_alloc(&p, sizeof(REAL) * NUM_EVOL_GFS * n));
   gridfuncs->y_n_gfs = (REAL*)p;
   gridfuncs->diagnostic_output_gfs = gridfuncs->y_nplus1_running_total_gfs;
 }
@@ -417,10 +420,10 @@ void MoL_free_memory_y_n_gfs(const paramstruct* params, MoL_gridfunctions_struct
 void MoL_malloc_non_y_n_gfs(const paramstruct* params, MoL_gridfunctions_struct* gridfuncs) {
   const size_t n = (size_t)params->Nxx_plus_2NGHOSTS0 * params->Nxx_plus_2NGHOSTS1 * params->Nxx_plus_2NGHOSTS2;
   void* p[4] = {nullptr, nullptr, nullptr, nullptr};
-  NRPYELL_CUDA(cudaMallocManaged(&p[0], sizeof(REAL) * NUM_EVOL_GFS * n));
-  NRPYELL_CUDA(cudaMallocManaged(&p[1], sizeof(REAL) * NUM_EVOL_GFS * n));
-  NRPYELL_CUDA(cudaMallocManaged(&p[2], sizeof(REAL) * NUM_EVOL_GFS * n));
-  NRPYELL_CUDA(cudaMallocManaged(&p[3], sizeof(REAL) * NUM_AUXEVOL_GFS * n));
+  NRPYELL_CUDA(managed_alloc(&p[0], sizeof(REAL) * NUM_EVOL_GFS * n));
+  NRPYELL_CUDA(managed_alloc(&p[1], sizeof(REAL) * NUM_EVOL_GFS * n));
+  NRPYELL_CUDA(managed_alloc(&p[2], sizeof(REAL) * NUM_EVOL_GFS * n));
+  NRPYELL_CUDA(managed_alloc(&p[3], sizeof(REAL) * NUM_AUXEVOL_GFS * n));
   gridfuncs->y_nplus1_running_total_gfs = (REAL*)p[0];
   gridfuncs->k_odd_gfs = (REAL*)p[1];
   gridfuncs->k_even_gfs = (REAL*)p[2];
@@ -593,7 +596,7 @@ int nrpyell_relax_mixed(griddata_struct* g, const REAL dt, const REAL log10_tol,
   const Dims d = su.d;
   const long long n2 = 2 * d.Ntot;
   FusedWork* w = su.w;
-  if (!w->f32) NRPYELL_CUDA(cudaMalloc(&w->f32, sizeof(float) * (4 * n2 + 3 * d.Ntot)));
+  if (!w->f32) NRPYELL_CUDA(dev_alloc(&w->f32, sizeof(float) * (4 * n2 + 3 * d.Ntot)));
   if (!status_ok()) return -1;
   StateBuffers b32;
   b32.y = w->f32;
@@ -650,7 +653,7 @@ int nrpyell_relax_host(const paramstruct* params, REAL* xx[3], const bc_struct* 
       cudaFree(g.gridfuncs.auxevol_gfs);
     }
     void* p[5];
-    for (int i = 0; i < 5; i++) NRPYELL_CUDA(cudaMalloc(&p[i], sizeof(REAL) * (i == 4 ? 3 : 2) * ntot));
+    for (int i = 0; i < 5; i++) NRPYELL_CUDA(dev_alloc(&p[i], sizeof(REAL) * (i == 4 ? 3 : 2) * ntot));
     g.gridfuncs.y_n_gfs = (REAL*)p[0];
     g.gridfuncs.y_nplus1_running_total_gfs = (REAL*)p[1];
     g.gridfuncs.k_odd_gfs = (REAL*)p[2];

@@ -26,6 +26,21 @@ void count_launch(int n = 1);
 long long launch_count();
 void set_launch_count(long long n);
 
+// Every device (and managed) allocation of the library goes through these,
+// so a caller can check through nrpyell_device_alloc_count that a call
+// allocated nothing.
+void count_alloc();
+template <typename T>
+inline cudaError_t dev_alloc(T** p, size_t bytes) {
+  count_alloc();
+  return cudaMalloc(reinterpret_cast<void**>(p), bytes);
+}
+template <typename T>
+inline cudaError_t managed_alloc(T** p, size_t bytes) {
+  count_alloc();
+  return cudaMallocManaged(reinterpret_cast<void**>(p), bytes);
+}
+
 #define NRPYELL_CUDA(call)                                                     \
   do {                                                                         \
     cudaError_t e_ = (call);                                                   \

@@ -23,7 +23,7 @@ FusedWork* get_work(const Dims& d, int history_len) {
         g_work_generation++;  // graphs captured with the old history are stale
         NRPYELL_CUDA(cudaStreamSynchronize(stream()));
         NRPYELL_CUDA(cudaFree(w->history));
-        NRPYELL_CUDA(cudaMalloc(&w->history, sizeof(double) * history_len));
+        NRPYELL_CUDA(dev_alloc(&w->history, sizeof(double) * history_len));
         w->history_len = history_len;
       }
       return w;
@@ -32,12 +32,12 @@ FusedWork* get_work(const Dims& d, int history_len) {
   w->d = d;
   w->tile[0] = w->tile[1] = -1;
   w->f32 = nullptr;
-  NRPYELL_CUDA(cudaMalloc(&w->state, sizeof(int) * 8 + sizeof(double) * 4));
+  NRPYELL_CUDA(dev_alloc(&w->state, sizeof(int) * 8 + sizeof(double) * 4));
   NRPYELL_CUDA(cudaMemset(w->state, 0, sizeof(int) * 8 + sizeof(double) * 4));
   w->zero_flag = w->state + 4;
   w->stall = (double*)(w->state + 8);
   w->history_len = history_len > 16 ? history_len : 16;
-  NRPYELL_CUDA(cudaMalloc(&w->history, sizeof(double) * w->history_len));
+  NRPYELL_CUDA(dev_alloc(&w->history, sizeof(double) * w->history_len));
   g_work.push_back(w);
   return w;
 }

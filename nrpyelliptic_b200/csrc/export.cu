@@ -148,7 +148,7 @@ extern "C" int nrpyell_interpolate_solution(const paramstruct* p, REAL* xx[3], c
   // one device block: points in, the four outputs (1 + 1 + 6 + 6 per point)
   double* buf = nullptr;
   const size_t n = (size_t)npts;
-  NRPYELL_CUDA(cudaMalloc(&buf, sizeof(double) * n * 17));
+  NRPYELL_CUDA(dev_alloc(&buf, sizeof(double) * n * 17));
   if (!status_ok()) return -1;
   double *d_xyz = buf, *d_uu = buf + 3 * n, *d_psi = buf + 4 * n, *d_g = buf + 5 * n, *d_K = buf + 11 * n;
   NRPYELL_CUDA(cudaMemcpyAsync(d_xyz, xyz, sizeof(double) * 3 * n, cudaMemcpyHostToDevice, stream()));

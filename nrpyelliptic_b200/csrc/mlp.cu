@@ -229,10 +229,10 @@ static Mlp* mlp_new(int n_in, int width, int depth, int n_out, int batch_max, un
     }
   }
   const size_t pb = sizeof(float) * q->n_params;
-  NRPYELL_CUDA(cudaMalloc(&q->p, pb));
-  NRPYELL_CUDA(cudaMalloc(&q->grad, pb));
-  NRPYELL_CUDA(cudaMalloc(&q->m, pb));
-  NRPYELL_CUDA(cudaMalloc(&q->v, pb));
+  NRPYELL_CUDA(dev_alloc(&q->p, pb));
+  NRPYELL_CUDA(dev_alloc(&q->grad, pb));
+  NRPYELL_CUDA(dev_alloc(&q->m, pb));
+  NRPYELL_CUDA(dev_alloc(&q->v, pb));
   NRPYELL_CUDA(cudaMemcpyAsync(q->p, host.data(), pb, cudaMemcpyHostToDevice, stream()));
   NRPYELL_CUDA(cudaMemsetAsync(q->m, 0, pb, stream()));
   NRPYELL_CUDA(cudaMemsetAsync(q->v, 0, pb, stream()));
@@ -240,15 +240,15 @@ static Mlp* mlp_new(int n_in, int width, int depth, int n_out, int batch_max, un
   if (n_in > wmax) wmax = n_in;
   for (int l = 0; l < L; l++) {
     float* b = nullptr;
-    NRPYELL_CUDA(cudaMalloc(&b, sizeof(float) * (size_t)batch_max * q->dims[l + 1]));
+    NRPYELL_CUDA(dev_alloc(&b, sizeof(float) * (size_t)batch_max * q->dims[l + 1]));
     q->h.push_back(b);
   }
-  NRPYELL_CUDA(cudaMalloc(&q->x, sizeof(float) * (size_t)batch_max * n_in));
-  NRPYELL_CUDA(cudaMalloc(&q->t, sizeof(float) * (size_t)batch_max * n_out));
-  NRPYELL_CUDA(cudaMalloc(&q->dbuf[0], sizeof(float) * (size_t)batch_max * wmax));
-  NRPYELL_CUDA(cudaMalloc(&q->dbuf[1], sizeof(float) * (size_t)batch_max * wmax));
-  NRPYELL_CUDA(cudaMalloc(&q->loss, sizeof(double)));
-  NRPYELL_CUDA(cudaMalloc(&q->idx, sizeof(int) * batch_max));
+  NRPYELL_CUDA(dev_alloc(&q->x, sizeof(float) * (size_t)batch_max * n_in));
+  NRPYELL_CUDA(dev_alloc(&q->t, sizeof(float) * (size_t)batch_max * n_out));
+  NRPYELL_CUDA(dev_alloc(&q->dbuf[0], sizeof(float) * (size_t)batch_max * wmax));
+  NRPYELL_CUDA(dev_alloc(&q->dbuf[1], sizeof(float) * (size_t)batch_max * wmax));
+  NRPYELL_CUDA(dev_alloc(&q->loss, sizeof(double)));
+  NRPYELL_CUDA(dev_alloc(&q->idx, sizeof(int) * batch_max));
   NRPYELL_CUDA(cudaStreamSynchronize(stream()));
   return q;
 }

@@ -20,8 +20,17 @@
 //     the start of every call.  Calls that overlap on the GPU (other threads
 //     or streams) race on the array and must be serialised by the caller.
 //   * The first call on each device looks up the array's device address with
-//     cudaGetSymbolAddress while that device is current; make that first call
-//     before any stream capture.
+//     cudaGetSymbolAddress while that device is current.  With lazy module
+//     loading (CUDA's default) that lookup also loads the library's GPU code,
+//     and the driver makes its own allocations for code and globals then:
+//     callers with a strict budget make the first call at start-up or run
+//     with CUDA_MODULE_LOADING=EAGER.
+//   * Every call copies xx0/xx1 from pageable host memory and waits for the
+//     result, so no call may be made while the stream it runs on (below) is
+//     being captured.
+//   * It runs on the library's stream when that stream belongs to the
+//     current device (ordering with earlier library calls), otherwise on the
+//     legacy default stream of the current device.
 //   * No cudaMalloc, cudaFree or other allocating routine is called.  The
 //     volume element is evaluated per point on the GPU (as L2_norm_of_gf.c
 //     does on the CPU) instead of coming from a cached weight table.
@@ -135,6 +144,11 @@ using namespace nrpyell;
 extern "C" REAL L2_norm_of_gf_noalloc(const paramstruct* params, const int gf_index, const REAL integration_radius,
                                       REAL* NRPYELL_RESTRICT xx[3], const REAL* in_gf) {
   const Dims d = dims_of(params);
+  if (d.N0 != d.Nxx0 + 2 * NGHOSTS || d.N1 != d.Nxx1 + 2 * NGHOSTS || d.N2 != d.Nxx2 + 2 * NGHOSTS || d.Nxx0 < 1 ||
+      d.Nxx1 < 1 || d.Nxx2 < 1) {
+    NRPYELL_FAIL("L2_norm_of_gf_noalloc: Nxx_plus_2NGHOSTSi must equal Nxxi + 2 NGHOSTS with Nxxi >= 1");
+    return NAN;
+  }
   if (d.N0 > kNoallocMaxN0 || d.N1 > kNoallocMaxN1) {
     char msg[200];
     snprintf(msg, sizeof(msg),
@@ -167,9 +181,14 @@ extern "C" REAL L2_norm_of_gf_noalloc(const paramstruct* params, const int gf_in
     g_noalloc_addr[dev] = (double*)p;
   }
   double* s = g_noalloc_addr[dev];
-  // The library's stream if it exists (ordering with earlier library calls),
-  // otherwise the default stream; no stream is created here.
+  // The library's stream if it exists and belongs to this device (ordering
+  // with earlier library calls), otherwise the default stream; no stream is
+  // created here.
   cudaStream_t st = existing_stream();
+  if (st) {
+    int sdev = -1;
+    if (cudaStreamGetDevice(st, &sdev) != cudaSuccess || sdev != dev) st = 0;
+  }
   NRPYELL_CUDA(cudaMemcpyAsync(s + kOffXX0, xx[0], sizeof(double) * d.N0, cudaMemcpyHostToDevice, st));
   NRPYELL_CUDA(cudaMemcpyAsync(s + kOffXX1, xx[1], sizeof(double) * d.N1, cudaMemcpyHostToDevice, st));
   NRPYELL_CUDA(cudaMemsetAsync(s + kOffTicket, 0, sizeof(double), st));

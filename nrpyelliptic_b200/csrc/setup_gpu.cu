@@ -79,7 +79,7 @@ extern "C" int nrpyell_auxevol_device(const paramstruct* p, REAL* xx[3], const R
     NRPYELL_CUDA(cudaStreamSynchronize(stream()));
     cudaFree(g_xx_dev);
     g_xx_dev = nullptr;
-    NRPYELL_CUDA(cudaMalloc(&g_xx_dev, sizeof(double) * nxx));
+    NRPYELL_CUDA(dev_alloc(&g_xx_dev, sizeof(double) * nxx));
     g_xx_cap = status_ok() ? nxx : 0;
   }
   if (!status_ok()) return -1;

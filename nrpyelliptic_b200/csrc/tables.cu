@@ -20,9 +20,9 @@ bool same_dims(const Dims& a, const Dims& b) {
   return a.N0 == b.N0 && a.N1 == b.N1 && a.N2 == b.N2 && a.Nxx0 == b.Nxx0 && a.Nxx1 == b.Nxx1 && a.Nxx2 == b.Nxx2;
 }
 
-void* dev_alloc(size_t bytes) {
+void* table_alloc(size_t bytes) {
   void* p = nullptr;
-  NRPYELL_CUDA(cudaMalloc(&p, bytes > 0 ? bytes : 16));
+  NRPYELL_CUDA(dev_alloc(&p, bytes > 0 ? bytes : 16));
   return p;
 }
 
@@ -100,7 +100,7 @@ RfmTables* get_rfm_tables(const paramstruct* p, const rfm_struct* rfm) {
   const size_t n0 = d.N0, n1 = d.N1, n01 = n0 * n1;
   const size_t n_doubles = 5 * n0 + 2 * n1 + 2 * n01 + kNumCoef * n01;
   const size_t bytes = n_doubles * sizeof(double) + kNumCoef * n01 * sizeof(float) + 256;
-  char* base = (char*)dev_alloc(bytes);
+  char* base = (char*)table_alloc(bytes);
   t->base = base;
   double* q = (double*)base;
   t->f0 = q; q += n0;
@@ -278,7 +278,7 @@ BcTables* get_bc_tables(const paramstruct* p, const bc_struct* bc, REAL* NRPYELL
   const size_t b_par = ((par.size() + 255) / 256) * 256;
   const size_t b_outer = (outer.size() > 0 ? outer.size() : 1) * sizeof(OuterPoint);
   const size_t b_col = colgeo.size() * sizeof(double);
-  char* base = (char*)dev_alloc(b_inner + b_par + b_outer + b_col + 1024);
+  char* base = (char*)table_alloc(b_inner + b_par + b_outer + b_col + 1024);
   t->base = base;
   size_t o = 0;
   t->inner = (int2*)(base + o); o += (b_inner + 255) / 256 * 256;
@@ -332,7 +332,7 @@ L2Tables* get_l2_tables(const paramstruct* p, REAL* NRPYELL_RESTRICT const xx[3]
       }
     }
   t->volume = (double)(vol * (long double)d.Nxx2);
-  t->w = (double*)dev_alloc(w.size() * sizeof(double));
+  t->w = (double*)table_alloc(w.size() * sizeof(double));
   upload(t->w, w.data(), w.size() * sizeof(double));
   g_l2.push_back(t);
   return t;
@@ -352,7 +352,7 @@ Scratch* get_scratch(int n_partials) {
   Scratch* s = new Scratch();
   s->n_partials = n_partials < 4096 ? 4096 : n_partials;
   const size_t bytes = (size_t)s->n_partials * 8 + 4 * 8 + 64 + 8 * 4 + 256;
-  char* base = (char*)dev_alloc(bytes);
+  char* base = (char*)table_alloc(bytes);
   NRPYELL_CUDA(cudaMemset(base, 0, bytes));
   s->base = base;
   s->partials = (double*)base;

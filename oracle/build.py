@@ -26,7 +26,9 @@ ROOT = os.path.dirname(HERE)
 INCLUDE = os.path.join(ROOT, "include")
 BUILD = os.path.join(HERE, "_build")
 REF_OUT = os.path.join(HERE, "_ref")
-REF_SRC = "/root/reference/NRPyElliptic_Ccodes"
+# The reference's C sources: NRPYELL_REFERENCE_SRC, else the read-only
+# checkout of this container.
+REF_SRC = os.environ.get("NRPYELL_REFERENCE_SRC", "/root/reference/NRPyElliptic_Ccodes")
 GPU_LIB_DIR = os.path.join(ROOT, "nrpyelliptic_b200")
 
 ORACLE_LIB = os.path.join(BUILD, "liboracle.so")

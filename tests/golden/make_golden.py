@@ -4,6 +4,8 @@ oracle/build.py from NRPyElliptic_Ccodes/*.c).
 
 Run in a checkout that has the reference sources:
     python tests/golden/make_golden.py
+    python tests/golden/make_golden.py --add-extrap   (only adds the
+        extrapolation-branch arrays to the existing ops_*.npz fixtures)
 
 Fixtures (numpy .npz):
   ops_<case>.npz      set-up outputs (params, xx, rfm tables, auxevol, dt,
@@ -11,7 +13,10 @@ Fixtures (numpy .npz):
                       function to a seeded random state: rhs_eval, the
                       radiation + inner BC, residual_all_points,
                       L2_norm_of_gf, 1 and 10 MoL steps, a 40-step
-                      residual history from the zero guess.
+                      residual history from the zero guess, and the
+                      extrapolation branch: apply_bcs_outerextrap_and_inner
+                      on the random state and one MoL step with
+                      outer_bc_type = EXTRAPOLATION_OUTER_BCS.
   relax_shipped_64x64x8.npz        full relaxation of the reference's shipped
                       puncture set to log10 L2 <= -10 (history + converged uu).
   relax_quasicircular_128x128x16.npz  relaxation of the quasi-circular pair to
@@ -166,6 +171,26 @@ def make_ops_case(lib, cfg, seed):
     out["relax_history40"] = hist
     out["y_relax40"] = arr(ydev, 2 * Ntot)
     lib.refh_free(C.byref(g))
+    out.update(extrap_case(lib, cfg, out["y_random"], out["y_consistent"]))
+    return out
+
+
+def extrap_case(lib, cfg, y_random, y_consistent):
+    """The extrapolation outer-BC branch of the reference
+    (apply_bcs_outerextrap_and_inner.c:15-75 and its call sites in
+    MoL_step_forward_in_time.c when outer_bc_type == EXTRAPOLATION_OUTER_BCS)."""
+    g, dt = setup(lib, cfg)
+    N, Ntot = dims(g)
+    out = {}
+    y = y_random.copy()
+    lib.apply_bcs_outerextrap_and_inner(C.byref(g.params), C.byref(g.bcstruct), y.ctypes.data_as(abi.PREAL))
+    out["y_extrap"] = y
+    g.params.outer_bc_type = abi.EXTRAPOLATION_OUTER_BCS
+    ydev = g.gridfuncs.y_n_gfs
+    C.memmove(ydev, y_consistent.ctypes.data, y_consistent.nbytes)
+    lib.MoL_step_forward_in_time(C.byref(g), dt)
+    out["y_step1_extrap"] = arr(ydev, 2 * Ntot)
+    lib.refh_free(C.byref(g))
     return out
 
 
@@ -200,15 +225,33 @@ def bcmap_digest(lib, cfg):
     return len(inner), counts, h, dt
 
 
-def main():
-    lib = load_ref("v4")
-    t0 = time.time()
-    cases = {
+def ops_cases():
+    return {
         "shipped_16x8x6": (Config("g", (16, 8, 6), SHIPPED_PUNCTURES, CFL=0.5), 1),
         "unequal_24x16x8": (Config("g", (24, 16, 8),
                                    Punctures(0.8, 0.2, (0, 0, 1.2), (0, 0, -4.8), (0, 0.06, 0), (0, -0.06, 0),
                                              (0, 0, 0.1), (0.05, 0, -0.03)), bScale=6.0), 2),
     }
+
+
+def add_extrap(lib):
+    """Adds the extrapolation-branch arrays to the existing ops fixtures
+    (same configurations, the fixtures' own random states)."""
+    for name, (cfg, _) in ops_cases().items():
+        path = os.path.join(OUT, "ops_%s.npz" % name)
+        d = dict(np.load(path))
+        d.update(extrap_case(lib, cfg, d["y_random"], d["y_consistent"]))
+        np.savez_compressed(path, **d)
+        print("extrap", name)
+
+
+def main():
+    lib = load_ref("v4")
+    if "--add-extrap" in sys.argv:
+        add_extrap(lib)
+        return
+    t0 = time.time()
+    cases = ops_cases()
     for name, (cfg, seed) in cases.items():
         d = make_ops_case(lib, cfg, seed)
         np.savez_compressed(os.path.join(OUT, "ops_%s.npz" % name), **d)

@@ -84,21 +84,39 @@ def test_radiation_bc_vs_reference(lib, case):
 
 
 @pytest.mark.parametrize("case", CASES)
-def test_inner_only_and_extrapolation_vs_oracle(lib, case):
+def test_inner_only_and_extrapolation_vs_reference(lib, case):
+    """apply_bcs_inner_only bit for bit and apply_bcs_outerextrap_and_inner
+    (apply_bcs_outerextrap_and_inner.c:15-75) against the reference build's
+    outputs on the same random state."""
     gold = load_golden(case)
     hg = golden_grid(gold)
-    o = oracle()
     y0 = gold["y_random"].copy()
     d = Dev(lib, y0)
     lib.apply_bcs_inner_only(C.byref(hg.params), C.byref(hg.bc), d.ptr)
     _lib.check(lib)
     np.testing.assert_array_equal(d.get(), gold["y_consistent"])
-    yo = y0.copy()
-    o.oracle_apply_bcs_outerextrap_and_inner(C.byref(hg.params), C.byref(hg.bc), ptr(yo))
     d.set(y0)
     lib.apply_bcs_outerextrap_and_inner(C.byref(hg.params), C.byref(hg.bc), d.ptr)
     _lib.check(lib)
-    assert relmax(d.get(), yo) < 1e-15
+    assert relmax(d.get(), gold["y_extrap"]) < 1e-15
+
+
+@pytest.mark.parametrize("mode", [0, 1])
+@pytest.mark.parametrize("case", CASES)
+def test_mol_step_extrapolation_bc_vs_reference(lib, case, mode):
+    """One MoL step with outer_bc_type = EXTRAPOLATION_OUTER_BCS: both step
+    modes take the reference-order path for this BC type."""
+    gold = load_golden(case)
+    hg = golden_grid(gold)
+    hg.params.outer_bc_type = abi.EXTRAPOLATION_OUTER_BCS
+    g, bufs = device_grid(lib, hg, gold["y_consistent"])
+    lib.nrpyell_set_step_mode(mode)
+    try:
+        lib.MoL_step_forward_in_time(C.byref(g), float(gold["dt"]))
+        _lib.check(lib)
+        assert relmax(bufs["y_n"].get(), gold["y_step1_extrap"]) < 1e-13
+    finally:
+        lib.nrpyell_set_step_mode(0)
 
 
 @pytest.mark.parametrize("mode,tol1,tol10", [(1, 1e-13, 1e-12), (0, 1e-12, 1e-12)])

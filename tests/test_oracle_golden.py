@@ -7,6 +7,7 @@ import numpy as np
 import pytest
 from _util import golden_grid, interior_mask, load_golden, oracle, problem_grid, ptr, relmax
 
+from nrpyelliptic_b200 import abi
 from nrpyelliptic_b200.problem import CONFIGS, Problem
 
 CASES = ["ops_shipped_16x8x6.npz", "ops_unequal_24x16x8.npz"]
@@ -71,6 +72,25 @@ def test_mol_steps(case):
     for _ in range(9):
         o.oracle_MoL_step_forward_in_time(C.byref(g), dt)
     assert relmax(hg.bufs["y_n"], gold["y_step10"]) < 1e-12
+
+
+@pytest.mark.parametrize("case", CASES)
+def test_extrapolation_branch(case):
+    """apply_bcs_outerextrap_and_inner (apply_bcs_outerextrap_and_inner.c:15-75)
+    on the random state, and one MoL step with outer_bc_type =
+    EXTRAPOLATION_OUTER_BCS (MoL_step_forward_in_time.c, extrapolation calls),
+    against the reference build's outputs."""
+    gold = load_golden(case)
+    hg = golden_grid(gold)
+    o = oracle()
+    y = gold["y_random"].copy()
+    o.oracle_apply_bcs_outerextrap_and_inner(C.byref(hg.params), C.byref(hg.bc), ptr(y))
+    assert relmax(y, gold["y_extrap"]) < 1e-15
+    hg.params.outer_bc_type = abi.EXTRAPOLATION_OUTER_BCS
+    hg.bufs["y_n"][:] = gold["y_consistent"]
+    g = hg.griddata()
+    o.oracle_MoL_step_forward_in_time(C.byref(g), float(gold["dt"]))
+    assert relmax(hg.bufs["y_n"], gold["y_step1_extrap"]) < 1e-13
 
 
 @pytest.mark.parametrize("case", CASES)

@@ -3,14 +3,19 @@ device memory (fixed-arena frameworks, processes under a device-memory quota,
 loops that cannot afford the synchronisation of cudaMalloc).  It is checked
 through the C ABI against the allocating L2_norm_of_gf on the same device
 data, on two calls in a row, within the L2 tolerance of the other parity tests
-(1e-13 in log10).  This file is collected last so that a stop at the first
-failure has already run every other test; it also passes on its own in a fresh
-process."""
+(1e-13 in log10), and the library's allocation counter is checked to stay
+unchanged across the no-allocation calls -- also in a fresh process whose very
+first library call is L2_norm_of_gf_noalloc.  This file is collected last so
+that a stop at the first failure has already run every other test; it also
+passes on its own in a fresh process."""
 import ctypes as C
+import os
+import subprocess
+import sys
 
 import numpy as np
 import pytest
-from _util import golden_grid, load_golden, problem_grid
+from _util import ROOT, golden_grid, load_golden, problem_grid
 
 from nrpyelliptic_b200 import _lib, abi
 from nrpyelliptic_b200.problem import CONFIGS, Problem
@@ -32,9 +37,11 @@ def _check_grid(lib, params, xx, residual):
     try:
         for R in (100.0, 1e300):
             ref = lib.L2_norm_of_gf(C.byref(params), abi.UUGF, R, xx, as_real)
+            allocs = lib.nrpyell_device_alloc_count()
             first = lib.L2_norm_of_gf_noalloc(C.byref(params), abi.UUGF, R, xx, as_real)
             second = lib.L2_norm_of_gf_noalloc(C.byref(params), abi.UUGF, R, xx, as_real)
             _lib.check(lib)
+            assert lib.nrpyell_device_alloc_count() == allocs
             assert np.isfinite(ref)
             assert abs(first - ref) <= TOL, (first, ref)
             assert abs(second - ref) <= TOL, (second, ref)
@@ -65,6 +72,44 @@ def test_noalloc_l2_matches_l2_norm_of_gf_on_production_grid():
     prob.close()
 
 
+_FRESH = r"""
+import ctypes as C, sys
+sys.path.insert(0, sys.argv[1]); sys.path.insert(0, sys.argv[1] + "/tests")
+import numpy as np
+from _util import golden_grid, load_golden
+from nrpyelliptic_b200 import _lib, abi
+lib = _lib.load()
+rt = C.CDLL("libcudart.so.12")  # the runtime the library is linked against
+gold = load_golden("ops_unequal_24x16x8.npz")
+hg = golden_grid(gold)
+res = np.zeros(2 * hg.Ntot)
+res[:hg.Ntot] = np.nan_to_num(gold["residual"])
+d = C.c_void_p()
+assert rt.cudaMalloc(C.byref(d), C.c_size_t(res.nbytes)) == 0
+assert rt.cudaMemcpy(d, res.ctypes.data_as(C.c_void_p), C.c_size_t(res.nbytes), 1) == 0
+p = C.cast(d, abi.PREAL)
+assert lib.nrpyell_device_alloc_count() == 0
+a = lib.L2_norm_of_gf_noalloc(C.byref(hg.params), abi.UUGF, 100.0, hg.xx, p)
+b = lib.L2_norm_of_gf_noalloc(C.byref(hg.params), abi.UUGF, 100.0, hg.xx, p)
+_lib.check(lib)
+assert lib.nrpyell_device_alloc_count() == 0, lib.nrpyell_device_alloc_count()
+ref = lib.L2_norm_of_gf(C.byref(hg.params), abi.UUGF, 100.0, hg.xx, p)
+_lib.check(lib)
+assert a == b and abs(a - ref) <= 1e-13 and abs(a - float(gold["l2_R100"])) <= 1e-13, (a, b, ref)
+print("fresh-process noalloc ok", a)
+"""
+
+
+def test_noalloc_l2_first_call_in_a_fresh_process_allocates_nothing():
+    """The first library call of a new process is the no-allocation norm: the
+    library's allocation counter stays at zero over two calls, and the
+    result equals L2_norm_of_gf's and the reference's."""
+    r = subprocess.run([sys.executable, "-c", _FRESH, ROOT], capture_output=True, text=True, timeout=600,
+                       env=dict(os.environ))
+    assert r.returncode == 0, r.stdout + r.stderr
+    assert "fresh-process noalloc ok" in r.stdout
+
+
 def test_noalloc_l2_rejects_grids_beyond_its_fixed_size():
     lib = _lib.load()
     lib.nrpyell_clear_status()
@@ -77,4 +122,11 @@ def test_noalloc_l2_rejects_grids_beyond_its_fixed_size():
     assert np.isnan(out)
     assert lib.nrpyell_last_status() != 0
     assert b"exceeds the fixed maximum" in lib.nrpyell_last_error()
+    lib.nrpyell_clear_status()
+    # padded sizes that disagree with Nxx + 2 NGHOSTS are rejected too
+    p.Nxx0, p.Nxx1, p.Nxx2 = 64, 64, 8
+    p.Nxx_plus_2NGHOSTS0, p.Nxx_plus_2NGHOSTS1, p.Nxx_plus_2NGHOSTS2 = 74, 80, 18
+    out = lib.L2_norm_of_gf_noalloc(C.byref(p), abi.UUGF, 100.0, xx, None)
+    assert np.isnan(out)
+    assert b"Nxx_plus_2NGHOSTS" in lib.nrpyell_last_error()
     lib.nrpyell_clear_status()
