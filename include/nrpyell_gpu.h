@@ -135,7 +135,9 @@ void nrpyell_set_async(int enable);
  * every shape on the caller's grid the first time a grid size is stepped
  * and keeps the fastest.  nrpyell_set_tile(t) forces shape t (-1: autotune);
  * nrpyell_get_tile reports the shape in use for a grid (block 32 x by threads,
- * `planes` consecutive i2 planes per thread), -1 if not tuned yet.
+ * `planes` consecutive i2 planes per thread), -1 if not tuned yet; its fp32
+ * argument selects FP64 (0), FP32 (1) or the FP32 correction form of
+ * nrpyell_relax_mixed (2, marching shapes only).
  * nrpyell_num_tiles gives the number of shapes; nrpyell_tile_info describes
  * shape t and returns -1 for an index out of range.  kind: 0 one thread per
  * (i0,i1) column of `planes` points reading its stencil through L1; 2 the
@@ -208,20 +210,28 @@ int nrpyell_auxevol_device(const paramstruct *params, REAL *xx[3], const REAL CF
 int nrpyell_relax(griddata_struct *griddata, const REAL dt, const REAL log10_tol, const int max_steps,
                   const REAL integration_radius, int *steps_taken, REAL *final_log10_l2, REAL *history);
 
-/* Mixed-precision relaxation: FP32 storage and arithmetic (the residual norm
- * accumulated in FP64) from the initial y_n until log10 L2 <= log10_switch or
- * the residual stalls -- its best value so far has not dropped below
- * stall_factor (e.g. 0.98) times itself for stall_window steps; the
- * relaxation residual oscillates, so only the running minimum counts, and
- * only once it is within two decades of log10_switch --
- * then FP64 from that state to
- * log10_tol.  steps_fp32 / steps_fp64 receive the RK4 steps of each phase;
- * history (nullable) log10 L2 per evaluated step (phase-2 values overwrite
- * the phase-1 value at the switch step).  Returns as nrpyell_relax. */
+/* Mixed-precision relaxation to log10 L2 <= log10_tol, main.c's stop test
+ * (residual before each step).  The state y_n stays FP64; the FP32 phase
+ * relaxes a correction to it (defect correction):
+ *   1. from the FP64 state U: its RHS with the radiation BC, its residual
+ *      bracket (residual_all_points) and log10 L2, all in FP64, and the
+ *      stop test on that norm;
+ *   2. an FP32 correction d starts at zero and takes up to fold_every RK4
+ *      steps of the same equations written for U + d, with U's FP64 RHS as a
+ *      fixed input, so FP32 rounding scales with d, not with U; its own
+ *      (FP32-evaluated) residual is tested against log10_switch each step;
+ *   3. U += d in FP64, and back to 1.
+ * Once the FP64 residual of U is <= log10_switch, or an FP32 stretch met
+ * log10_switch by its own evaluation or made no progress, FP64 RK4 steps
+ * (the plain fused kernels) continue from U to log10_tol.  log10_switch =
+ * log10_tol keeps every step in FP32, with the FP64 norm as the judge.
+ * steps_fp32 / steps_fp64 receive the RK4 steps of each phase; history
+ * (nullable) log10 L2 per step (FP64 values at the fold steps, the FP32
+ * evaluation in between).  1 <= fold_every <= 4096; grids with
+ * 3 Ntot >= 2^32 are rejected.  Returns as nrpyell_relax. */
 int nrpyell_relax_mixed(griddata_struct *griddata, const REAL dt, const REAL log10_tol, const REAL log10_switch,
-                        const int stall_window, const REAL stall_factor, const int max_steps,
-                        const REAL integration_radius, int *steps_fp32, int *steps_fp64, REAL *final_log10_l2,
-                        REAL *history);
+                        const int fold_every, const int max_steps, const REAL integration_radius, int *steps_fp32,
+                        int *steps_fp64, REAL *final_log10_l2, REAL *history);
 
 /* The same relaxation with the stopping rule of the Einstein Toolkit thorn
  * (NRPyEllipticET_conformally_flat_BBH_Hyperbolic_Relaxation.c:185-217):

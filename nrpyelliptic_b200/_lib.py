@@ -79,8 +79,7 @@ EXPORTS = {
     "nrpyell_relax": (C.c_int, [P(abi.griddata_struct), C.c_double, C.c_double, C.c_int, C.c_double, P(C.c_int),
                                 P(C.c_double), PREAL]),
     "nrpyell_relax_mixed": (C.c_int, [P(abi.griddata_struct), C.c_double, C.c_double, C.c_double, C.c_int,
-                                      C.c_double, C.c_int, C.c_double, P(C.c_int), P(C.c_int), P(C.c_double),
-                                      PREAL]),
+                                      C.c_int, C.c_double, P(C.c_int), P(C.c_int), P(C.c_double), PREAL]),
     "nrpyell_relax_et": (C.c_int, [P(abi.griddata_struct), C.c_double, C.c_double, C.c_int, C.c_int, C.c_double,
                                    P(C.c_int), P(C.c_double)]),
     "nrpyell_compute_TRC": (C.c_double, [C.c_double] * 6),

@@ -177,6 +177,9 @@ struct RelaxSetup {
   Scratch* s;
 };
 
+// Longest FP32 stretch of nrpyell_relax_mixed between two folds.
+constexpr int kMaxFoldEvery = 4096;
+
 static int relax_prepare(griddata_struct* g, int max_steps, double R, RelaxSetup* out, const char* who) {
   char msg[256];
   if (max_steps < 0) {
@@ -583,58 +586,111 @@ void nrpyell_set_optimum_eta_damping(const REAL dt, const REAL CFL_FACTOR, param
 }
 
 int nrpyell_relax_mixed(griddata_struct* g, const REAL dt, const REAL log10_tol, const REAL log10_switch,
-                        const int stall_window, const REAL stall_factor, const int max_steps,
-                        const REAL integration_radius, int* steps_fp32, int* steps_fp64, REAL* final_log10_l2,
-                        REAL* history) {
+                        const int fold_every, const int max_steps, const REAL integration_radius, int* steps_fp32,
+                        int* steps_fp64, REAL* final_log10_l2, REAL* history) {
   RelaxSetup su;
   const int rc = relax_prepare(g, max_steps, integration_radius, &su, "nrpyell_relax_mixed");
   if (rc) return rc;
-  if (!(stall_factor > 0.0 && stall_factor < 1.0) || stall_window < 0) {
-    NRPYELL_FAIL("nrpyell_relax_mixed: need 0 < stall_factor < 1 and stall_window >= 0");
+  if (fold_every < 1 || fold_every > kMaxFoldEvery) {
+    NRPYELL_FAIL("nrpyell_relax_mixed: need 1 <= fold_every <= 4096");
+    return -1;
+  }
+  if (!march_fits(su.d)) {
+    NRPYELL_FAIL("nrpyell_relax_mixed: grid too large for the FP32 correction kernels (3 Ntot >= 2^32)");
     return -1;
   }
   const Dims d = su.d;
   const long long n2 = 2 * d.Ntot;
   FusedWork* w = su.w;
-  if (!w->f32) NRPYELL_CUDA(dev_alloc(&w->f32, sizeof(float) * (4 * n2 + 3 * d.Ntot)));
+  if (!w->f32) NRPYELL_CUDA(dev_alloc(&w->f32, sizeof(float) * (6 * n2 + 3 * d.Ntot)));
+  const int cycle_len = std::min(fold_every, max_steps);
+  if (!w->cycle_history) NRPYELL_CUDA(dev_alloc(&w->cycle_history, sizeof(double) * (kMaxFoldEvery + 1)));
   if (!status_ok()) return -1;
+  // FP32 buffers: the correction and its RK buffers, the pointwise fields,
+  // the base state's RHS
   StateBuffers b32;
   b32.y = w->f32;
   b32.acc = w->f32 + n2;
   b32.kodd = w->f32 + 2 * n2;
   b32.keven = w->f32 + 3 * n2;
   b32.aux = w->f32 + 4 * n2;
-  const StateBuffers b64 = buffers_of(&g->gridfuncs);
-  // Phase 1: FP32 storage and arithmetic (residual norm accumulated in FP64)
-  // until log10 L2 <= log10_switch or the residual stalls.
-  convert_to_float(g->gridfuncs.auxevol_gfs, (float*)b32.aux, 3 * d.Ntot);
-  convert_to_float(g->gridfuncs.y_n_gfs, (float*)b32.y, n2);
-  RelaxParams rp = relax_params(&g->params, dt);
+  b32.R0 = w->f32 + 4 * n2 + 3 * d.Ntot;
+  MoL_gridfunctions_struct* gf = &g->gridfuncs;
+  double* U = gf->y_n_gfs;
+  double* rhs64 = gf->k_odd_gfs;                   // scratch of the FP64 base evaluation
+  double* res64 = gf->y_nplus1_running_total_gfs;  // (both are overwritten by every RK4 step)
+  const StateBuffers b64 = buffers_of(gf);
+  const paramstruct* p = &g->params;
+  const double cw[2] = {p->uu_wavespeed_at_OB, p->vv_wavespeed_at_OB};
+  const double finf[2] = {0.0, 0.0};
+
+  RelaxParams rp = relax_params(p, dt);
   rp.log10_tol = log10_switch;
-  rp.max_steps = max_steps;
-  rp.stall_window = stall_window;
-  rp.stall_log_drop = log10(stall_factor);
-  const int tile32 = tuned_tile<float>(d, su.rt, su.bt, w, su.s, b32, rp);
-  const RelaxResult r32 = relax_loop<float>(d, su.rt, su.bt, su.lt, w, su.s, tile32, b32, rp);
-  if (!status_ok()) return -1;
-  // Phase 2: FP64 from the FP32 state to the final tolerance.
-  convert_to_double((const float*)b32.y, g->gridfuncs.y_n_gfs, n2);
-  RelaxParams rp64 = relax_params(&g->params, dt);
-  rp64.log10_tol = log10_tol;
-  rp64.max_steps = max_steps - r32.steps;
-  rp64.history_offset = r32.steps;
-  const int tile64 = tuned_tile<double>(d, su.rt, su.bt, w, su.s, b64, rp64);
-  const RelaxResult r64 = relax_loop<double>(d, su.rt, su.bt, su.lt, w, su.s, tile64, b64, rp64);
-  launch_ghost_fill<double>(d, su.bt, g->gridfuncs.y_n_gfs);
+  rp.history_buf = w->cycle_history;
+  int n = 0, tile32 = -1;
+  bool converged = false, to_fp64 = false;
+  double l2 = NAN;
+  for (;;) {
+    // FP64 evaluation of the base state: its ghost zones, RHS with the
+    // radiation BC, residual and L2 norm (the stop test), then the FP32
+    // inputs of the correction kernels.
+    launch_ghost_fill<double>(d, su.bt, U);
+    launch_rhs_ref(d, p, su.rt, gf->auxevol_gfs, U, rhs64);
+    launch_radiation_bc(d, p, su.bt, cw, finf, U, rhs64);
+    launch_residual_ref(d, su.rt, gf->auxevol_gfs, U, res64);
+    launch_l2_sum(d, su.lt, res64, su.s);
+    launch_correction_base(d, U, gf->auxevol_gfs, rhs64, res64, (float*)b32.R0, (float*)b32.aux);
+    double sum = 0.0;
+    NRPYELL_CUDA(cudaMemcpyAsync(&sum, su.s->result, sizeof(double), cudaMemcpyDeviceToHost, stream()));
+    NRPYELL_CUDA(cudaStreamSynchronize(stream()));
+    if (!status_ok()) return -1;
+    l2 = log10(1e-16 + sqrt(sum / su.lt->volume));
+    NRPYELL_CUDA(cudaMemcpy(w->history + n, &l2, sizeof(double), cudaMemcpyHostToDevice));
+    if (l2 <= log10_tol) {
+      converged = true;
+      break;
+    }
+    if (l2 <= log10_switch || to_fp64 || n >= max_steps) break;
+    // One FP32 stretch: the correction relaxes from zero for up to
+    // fold_every steps, or until its FP32-evaluated residual reaches
+    // log10_switch, and is folded into U.
+    NRPYELL_CUDA(cudaMemsetAsync(b32.y, 0, sizeof(float) * n2, stream()));
+    rp.max_steps = std::min(cycle_len, max_steps - n);
+    if (tile32 < 0) tile32 = tuned_tile<float>(d, su.rt, su.bt, w, su.s, b32, rp);
+    const RelaxResult r = relax_loop<float>(d, su.rt, su.bt, su.lt, w, su.s, tile32, b32, rp);
+    if (!status_ok()) return -1;
+    launch_correction_fold(U, (const float*)b32.y, n2);
+    if (r.steps > 0)
+      NRPYELL_CUDA(cudaMemcpyAsync(w->history + n + 1, w->cycle_history + 1, sizeof(double) * r.steps,
+                                   cudaMemcpyDeviceToDevice, stream()));
+    n += r.steps;
+    // the FP32 evaluation met the switch tolerance (the FP64 one decides at
+    // the top of the loop) or made no progress: the FP64 phase takes over
+    if (r.converged || r.steps == 0) to_fp64 = true;
+  }
+  const int n32 = n;
+  int n64 = 0;
+  if (!converged && n < max_steps && status_ok()) {
+    RelaxParams rp64 = relax_params(p, dt);
+    rp64.log10_tol = log10_tol;
+    rp64.max_steps = max_steps - n;
+    rp64.history_offset = n;
+    const int tile64 = tuned_tile<double>(d, su.rt, su.bt, w, su.s, b64, rp64);
+    const RelaxResult r64 = relax_loop<double>(d, su.rt, su.bt, su.lt, w, su.s, tile64, b64, rp64);
+    n64 = r64.steps;
+    converged = r64.converged;
+    l2 = r64.last_log10_l2;
+  }
+  launch_ghost_fill<double>(d, su.bt, U);
   if (history)
-    NRPYELL_CUDA(cudaMemcpyAsync(history, w->history, sizeof(double) * (r32.steps + r64.steps + 1),
-                                 cudaMemcpyDeviceToHost, stream()));
+    NRPYELL_CUDA(cudaMemcpyAsync(history, w->history, sizeof(double) * (n32 + n64 + 1), cudaMemcpyDeviceToHost,
+                                 stream()));
   NRPYELL_CUDA(cudaStreamSynchronize(stream()));
   if (!status_ok()) return -1;
-  if (steps_fp32) *steps_fp32 = r32.steps;
-  if (steps_fp64) *steps_fp64 = r64.steps;
-  if (final_log10_l2) *final_log10_l2 = r64.last_log10_l2;
-  return r64.converged ? 0 : 1;
+  if (steps_fp32) *steps_fp32 = n32;
+  if (steps_fp64) *steps_fp64 = n64;
+  if (final_log10_l2) *final_log10_l2 = l2;
+  return converged ? 0 : 1;
 }
 
 int nrpyell_relax_host(const paramstruct* params, REAL* xx[3], const bc_struct* bcstruct, const rfm_struct* rfmstruct,

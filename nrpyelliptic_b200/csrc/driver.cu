@@ -30,8 +30,9 @@ FusedWork* get_work(const Dims& d, int history_len) {
     }
   FusedWork* w = new FusedWork();
   w->d = d;
-  w->tile[0] = w->tile[1] = -1;
+  w->tile[0] = w->tile[1] = w->tile[2] = -1;
   w->f32 = nullptr;
+  w->cycle_history = nullptr;
   NRPYELL_CUDA(dev_alloc(&w->state, sizeof(int) * 8 + sizeof(double) * 4));
   NRPYELL_CUDA(cudaMemset(w->state, 0, sizeof(int) * 8 + sizeof(double) * 4));
   w->zero_flag = w->state + 4;
@@ -47,6 +48,7 @@ void release_work() {
     cudaFree(w->state);
     cudaFree(w->history);
     if (w->f32) cudaFree(w->f32);
+    if (w->cycle_history) cudaFree(w->cycle_history);
     delete w;
   }
   g_work.clear();
@@ -54,7 +56,7 @@ void release_work() {
 
 int find_tile(const Dims& d, int fp32) {
   for (FusedWork* w : g_work)
-    if (w->d.N0 == d.N0 && w->d.N1 == d.N1 && w->d.N2 == d.N2) return w->tile[fp32 ? 1 : 0];
+    if (w->d.N0 == d.N0 && w->d.N1 == d.N1 && w->d.N2 == d.N2) return w->tile[fp32 >= 0 && fp32 <= 2 ? fp32 : 0];
   return -1;
 }
 
@@ -78,6 +80,7 @@ StateBuffers buffers_of(const MoL_gridfunctions_struct* gf) {
   b.kodd = gf->k_odd_gfs;
   b.keven = gf->k_even_gfs;
   b.aux = gf->auxevol_gfs;
+  b.R0 = nullptr;
   return b;
 }
 
@@ -94,6 +97,7 @@ SubstepArgs substep_args(const Dims& d, RfmTables* rt, BcTables* bt, Scratch* s,
   a.y = b.y;
   a.acc = b.acc;
   a.aux = b.aux;
+  a.R0 = b.R0;
   a.dt = rp.dt;
   a.eta = rp.eta;
   a.cOB[0] = rp.cOB[0];
@@ -126,19 +130,22 @@ SubstepArgs substep_args(const Dims& d, RfmTables* rt, BcTables* bt, Scratch* s,
 template <typename T>
 int tuned_tile(const Dims& d, RfmTables* rt, BcTables* bt, FusedWork* w, Scratch* sc, const StateBuffers& b,
                const RelaxParams& rp) {
-  const int which = sizeof(T) == 8 ? 0 : 1;
-  if (g_forced_tile >= 0) return g_forced_tile;
+  // the correction form runs on the marching shapes only
+  const bool corr = b.R0 != nullptr;
+  const int which = sizeof(T) == 8 ? 0 : (corr ? 2 : 1);
+  if (g_forced_tile >= 0 && !(corr && substep_tile_kind(g_forced_tile) != 5)) return g_forced_tile;
   if (w->tile[which] >= 0) return w->tile[which];
   cudaEvent_t e0, e1;
   NRPYELL_CUDA(cudaEventCreate(&e0));
   NRPYELL_CUDA(cudaEventCreate(&e1));
-  int best = 0;
+  int best = -1;
   float best_ms = 1e30f;
   // Each shape is timed on stages 1-3 back to back, as a relaxation runs
   // them (a shape can be fast at one stage and slow at the next); stage 4
   // would write y_n, the caller's state, so it is left out -- stages 1-3
   // write only the running total and the stage buffers.
   for (int t = 0; t < substep_num_tiles(); t++) {
+    if (corr && (substep_tile_kind(t) != 5 || !march_fits(d))) continue;
     SubstepArgs a[3];
     for (int st = 1; st <= 3; st++) a[st - 1] = substep_args(d, rt, bt, sc, b, rp, st, w->zero_flag, w->state, t);
     prepare_substep<T>(t);
@@ -161,6 +168,10 @@ int tuned_tile(const Dims& d, RfmTables* rt, BcTables* bt, FusedWork* w, Scratch
   }
   NRPYELL_CUDA(cudaEventDestroy(e0));
   NRPYELL_CUDA(cudaEventDestroy(e1));
+  if (best < 0) {
+    NRPYELL_FAIL("tile autotuner: no tile shape runs this form on this grid");
+    return 0;
+  }
   w->tile[which] = best;
   return best;
 }
@@ -227,7 +238,7 @@ RelaxResult relax_loop(const Dims& d, RfmTables* rt, BcTables* bt, L2Tables* lt,
       // stage 1 also evaluates the residual of y_n and runs the stop test
       SubstepArgs a1 = substep_args(d, rt, bt, s, b, rp, 1, w->state + 1, w->state, tile);
       a1.lt = lt;
-      a1.history = w->history + rp.history_offset;
+      a1.history = (rp.history_buf ? rp.history_buf : w->history) + rp.history_offset;
       a1.log10_tol = rp.log10_tol;
       a1.max_steps = rp.max_steps;
       a1.check_every = rp.check_every;
@@ -301,14 +312,46 @@ RelaxResult relax_loop(const Dims& d, RfmTables* rt, BcTables* bt, L2Tables* lt,
   res.steps = st[0];
   res.converged = st[2] != 0;
   res.stalled = st[3] != 0;
-  NRPYELL_CUDA(cudaMemcpy(&res.last_log10_l2, w->history + rp.history_offset + st[0], sizeof(double),
-                          cudaMemcpyDeviceToHost));
+  NRPYELL_CUDA(cudaMemcpy(&res.last_log10_l2, (rp.history_buf ? rp.history_buf : w->history) + rp.history_offset + st[0],
+                          sizeof(double), cudaMemcpyDeviceToHost));
   return res;
 }
 template RelaxResult relax_loop<double>(const Dims&, RfmTables*, BcTables*, L2Tables*, FusedWork*, Scratch*, int,
                                         const StateBuffers&, const RelaxParams&);
 template RelaxResult relax_loop<float>(const Dims&, RfmTables*, BcTables*, L2Tables*, FusedWork*, Scratch*, int,
                                        const StateBuffers&, const RelaxParams&);
+
+__global__ void k_correction_base(Dims d, const double* __restrict__ U, const double* __restrict__ aux,
+                                  const double* __restrict__ rhs, const double* __restrict__ res, float* __restrict__ R0,
+                                  float* __restrict__ aux32) {
+  const long long n = d.Ntot;
+  for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
+    const int i0 = (int)(i % d.N0);
+    const long long q = i / d.N0;
+    const int i1 = (int)(q % d.N1), i2 = (int)(q / d.N1);
+    const bool interior = i0 >= NGHOSTS && i0 < NGHOSTS + d.Nxx0 && i1 >= NGHOSTS && i1 < NGHOSTS + d.Nxx1 &&
+                          i2 >= NGHOSTS && i2 < NGHOSTS + d.Nxx2;
+    const double P = aux[PSI_BACKGROUNDGF * n + i] + U[i];
+    const double P2 = P * P, P4 = P2 * P2, P7 = P4 * P2 * P;
+    R0[i] = (float)rhs[i];
+    R0[n + i] = (float)(interior ? res[i] : rhs[n + i]);
+    aux32[ADD_TIMES_AUUGF * n + i] = (float)(0.125 * aux[ADD_TIMES_AUUGF * n + i] / P7);
+    aux32[PSI_BACKGROUNDGF * n + i] = (float)P;
+    aux32[WAVESPEEDGF * n + i] = (float)aux[WAVESPEEDGF * n + i];
+  }
+}
+void launch_correction_base(const Dims& d, const double* U, const double* aux, const double* rhs, const double* res,
+                            float* R0, float* aux32) {
+  NRPYELL_LAUNCH(k_correction_base, 148 * 8, 256, 0, d, U, aux, rhs, res, R0, aux32);
+}
+
+__global__ void k_correction_fold(double* __restrict__ U, const float* __restrict__ c, long long n) {
+  for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
+    U[i] += (double)c[i];
+}
+void launch_correction_fold(double* U, const float* corr, long long n) {
+  NRPYELL_LAUNCH(k_correction_fold, 148 * 8, 256, 0, U, corr, n);
+}
 
 __global__ void k_to_float(const double* __restrict__ in, float* __restrict__ out, long long n) {
   const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;

@@ -16,9 +16,12 @@ struct FusedWork {
   double* stall;   // [0] log10 L2 at the start of the stall window, [1] its step
   double* history;
   int history_len;
-  int tile[2];     // autotuned tile for FP64 / FP32, -1 = not tuned yet
-  // FP32 copies of the state for the mixed-precision driver (allocated on demand)
-  float* f32;      // y, acc, k_odd, k_even (2 gfs each) and aux (3 gfs)
+  int tile[3];     // autotuned tile for FP64 / FP32 / FP32 correction form, -1 = not tuned yet
+  // FP32 buffers of the mixed-precision driver (allocated on demand): the
+  // correction and its RK buffers y, acc, k_odd, k_even (2 gfs each), the
+  // pointwise fields (3 gfs) and the base state's RHS R0 (2 gfs)
+  float* f32;
+  double* cycle_history;  // residual history of one FP32 stretch
 };
 
 // Gridfunction buffers of one precision (T = double or float).
@@ -28,6 +31,7 @@ struct StateBuffers {
   void* kodd;
   void* keven;
   const void* aux;
+  const void* R0;  // correction form (SubstepArgs::R0), else nullptr
 };
 
 struct RelaxParams {
@@ -38,6 +42,7 @@ struct RelaxParams {
   int stall_window;       // 0: no stall test
   double stall_log_drop;  // stalled when log10 L2 fell by less than this over the window (negative)
   int history_offset;     // history index of step 0 of this run
+  double* history_buf;    // where the history goes (nullptr: the work's own)
 };
 
 struct RelaxResult {
@@ -68,6 +73,16 @@ int tuned_tile(const Dims& d, RfmTables* rt, BcTables* bt, FusedWork* w, Scratch
 template <typename T>
 RelaxResult relax_loop(const Dims& d, RfmTables* rt, BcTables* bt, L2Tables* lt, FusedWork* w, Scratch* s, int tile,
                        const StateBuffers& b, const RelaxParams& rp);
+// Correction form of the mixed-precision driver (nrpyell_relax_mixed): from
+// the FP64 base state U, its RHS rhs (interior and radiation ghost points)
+// and its residual bracket res (interior), the FP32 inputs of the correction
+// kernels: R0 = (uu RHS; bracket at interior points, vv RHS elsewhere) and
+// aux32 = (S(U) = ADD_times_AUU / (8 P^7), P = psi_background + U,
+// wavespeed), over all points.
+void launch_correction_base(const Dims& d, const double* U, const double* aux, const double* rhs, const double* res,
+                            float* R0, float* aux32);
+// U += correction over n values (both gridfunctions, all points).
+void launch_correction_fold(double* U, const float* corr, long long n);
 // Elementwise precision conversions on the library stream.
 void convert_to_float(const double* in, float* out, long long n);
 void convert_to_double(const float* in, double* out, long long n);

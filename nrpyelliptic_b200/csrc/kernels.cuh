@@ -29,6 +29,10 @@ struct SubstepArgs {
   void* acc;          // running total
   void* out;          // stage output (next stage input, or y_n at stage 4)
   const void* aux;    // auxevol (ADD_times_AUU, psi_background, wavespeed)
+  // Correction form (FP32 only, marching shapes only): the base state's RHS
+  // (see point_rhs_correction); aux then holds (S(U), psi + U, wavespeed).
+  // nullptr: the plain form.
+  const void* R0;
   double dt, eta, cOB[2];
   const RfmTables* rt;
   const BcTables* bt;

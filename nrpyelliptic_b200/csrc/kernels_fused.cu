@@ -546,6 +546,10 @@ static void launch_tile(const SubstepArgs& a) {
 
 template <typename T>
 void launch_substep(int stage, const SubstepArgs& a) {
+  if (a.R0 && (sizeof(T) != 4 || kTiles[a.tile].kind != 5)) {
+    NRPYELL_FAIL("launch_substep: the correction form runs on FP32 marching shapes only");
+    return;
+  }
   const bool resid = (stage == 1) && a.lt;
   switch (stage) {
     case 1:

@@ -53,30 +53,33 @@ __device__ __forceinline__ void cp_async_wait() {
 // Shared memory of one block, in elements of T per ring slot: the widened uu
 // plane [BY+10][42], then NPF pointwise rows of NT values (vv, ADD_TIMES_AUU,
 // psi_background, wavespeed, y_n uu, y_n vv, uu at i2+5, and from stage 2 on
-// the running totals of uu and vv).  Rows of 42 doubles are 336 bytes, so
-// every row starts on a 16-byte boundary.  (The pointwise fields are copied
-// per point: 16-byte pieces of their rows, from i0 = i00-1, were slower.)
-template <typename T, int BY, int STAGE, int D>
+// the running totals of uu and vv, and in the correction form R0u and R0b as
+// the last two rows).  Rows of 42 doubles are 336 bytes, so every row starts
+// on a 16-byte boundary.  (The pointwise fields are copied per point: 16-byte
+// pieces of their rows, from i0 = i00-1, were slower.)
+template <typename T, int BY, int STAGE, int D, bool CORR = false>
 struct MarchSmem {
   static constexpr int NT = 32 * BY, NR = BY + 10, RWS = 42;
-  static constexpr int NPF = STAGE == 1 ? 7 : 9;
+  static constexpr int NPF = (STAGE == 1 ? 7 : 9) + (CORR ? 2 : 0);
   static constexpr int plane = NR * RWS;
   static constexpr int slot = plane + NPF * NT;
   static constexpr size_t march = (size_t)D * slot * sizeof(T);
-  static constexpr size_t bytes = march > sizeof(double) * kRowsSmem ? march : sizeof(double) * kRowsSmem;
+  static constexpr size_t cols = sizeof(double) * (CORR ? kRowsSmemCorr : kRowsSmem);
+  static constexpr size_t bytes = march > cols ? march : cols;
 };
 
 // Block `bid` of one grid's marching launch; dsm is the block's dynamic
 // shared memory (MarchSmem::bytes).  The radiation column blocks come after
 // the interior blocks (COLS_LAST: their short, latency-bound blocks fill the
 // last wave's free slots) or before them (the batched launch's per-grid
-// block ranges).
-template <typename T, int STAGE, bool RESID, int BY, int PZ, int D, bool COLS_LAST>
+// block ranges).  CORR: the correction form (point_rhs_correction; a.R0 and
+// the correction's pointwise fields).
+template <typename T, int STAGE, bool RESID, int BY, int PZ, int D, bool COLS_LAST, bool CORR = false>
 __device__ __forceinline__ void march_block(const SubDev<T>& a, const int bid, double* dsm, double* sh, bool* lastp) {
-  using L = MarchSmem<T, BY, STAGE, D>;
+  using L = MarchSmem<T, BY, STAGE, D, CORR>;
   constexpr int NT = L::NT, NR = L::NR, RWS = L::RWS, HALF = RWS / 2;
   if (COLS_LAST ? bid >= a.n_tiles : bid < a.n_col_blocks) {
-    column_rows<T, STAGE, NT>(a, COLS_LAST ? bid - a.n_tiles : bid, dsm);
+    column_rows<T, STAGE, NT, CORR>(a, COLS_LAST ? bid - a.n_tiles : bid, dsm);
     return;
   }
   T* const ring = reinterpret_cast<T*>(dsm);
@@ -105,17 +108,18 @@ __device__ __forceinline__ void march_block(const SubDev<T>& a, const int bid, d
     return wrapm(j, Nxx2);
   };
   // tiles whose widened planes reach an inner ghost zone gather each point
-  // from its source; the others copy rows (16-byte pieces for FP64 when the
-  // rows are 16-byte aligned: N0 even and an aligned array)
+  // from its source; the others copy rows in pieces of two elements (16
+  // bytes for FP64, 8 for FP32) when the pieces are aligned: N0 even and an
+  // aligned array
   const bool inner = (t0 == 0) || (i10 < 2 * NGHOSTS) || (i10 + BY + NGHOSTS > top);
-  const bool vec = sizeof(T) == 8 && !inner && (N0 & 1) == 0 && (reinterpret_cast<size_t>(u) & 15) == 0;
+  const bool vec = !inner && (N0 & 1) == 0 && (reinterpret_cast<size_t>(u) & (2 * sizeof(T) - 1)) == 0;
   const int i0 = i00 + tx, i1 = i10 + ty;
   const bool valid = i0 < NGHOSTS + a.Nxx0 && i1 < top;
   const unsigned k2 = (unsigned)(i0 + N0 * i1);
   // at stage 1 the stage input is y_n itself: y_n's uu and vv at the point
   // are the plane's centre value and the vv already copied
   const bool y_is_s = STAGE == 1 && a.y == a.S;
-  // the 16-byte pieces of a widened plane this thread copies: offsets within
+  // the two-element pieces of a widened plane this thread copies: offsets within
   // the plane (global, without the plane term) and in the slot; the same for
   // every plane
   constexpr int NV = (NR * HALF + NT - 1) / NT;
@@ -141,7 +145,7 @@ __device__ __forceinline__ void march_block(const SubDev<T>& a, const int bid, d
       if (vec) {
 #pragma unroll
         for (int v = 0; v < NV; v++)
-          if (vs[v] >= 0) cp_async<16>(su + vs[v], u + (vg[v] + pl));
+          if (vs[v] >= 0) cp_async<2 * (int)sizeof(T)>(su + vs[v], u + (vg[v] + pl));
       } else {
         const unsigned plh = N01 * (unsigned)wrap2(i2 + a.half2, Nxx2);
         for (int e = tid; e < NR * RWS; e += NT) {
@@ -179,6 +183,10 @@ __device__ __forceinline__ void march_block(const SubDev<T>& a, const int bid, d
         if (STAGE != 1) {
           cp_async<(int)sizeof(T)>(pf + 7 * NT + tid, a.acc + idx);
           cp_async<(int)sizeof(T)>(pf + 8 * NT + tid, a.acc + (idx + Ntot));
+        }
+        if (CORR) {
+          cp_async<(int)sizeof(T)>(pf + (L::NPF - 2) * NT + tid, a.R0 + idx);
+          cp_async<(int)sizeof(T)>(pf + (L::NPF - 1) * NT + tid, a.R0 + (idx + Ntot));
         }
       }
     }
@@ -227,8 +235,15 @@ __device__ __forceinline__ void march_block(const SubDev<T>& a, const int bid, d
 #pragma unroll
       for (int k = 1; k <= 5; k++) s22 = fma(W<T>::e(k), q[p + 5 + k] + q[p + 5 - k], s22);
       T ku, kv, br;
-      point_rhs<T>(q[p + 5], pf[0], pf[NT], pf[2 * NT], pf[3 * NT], C22, C00, C11, C1, C0, Cc, s0, s1, s00, s11, s22,
-                   a.eta, ku, kv, br);
+      if (CORR) {
+        T ju, jv;
+        point_rhs_correction<T>(q[p + 5], pf[0], pf[NT], pf[2 * NT], pf[3 * NT], C22, C00, C11, C1, C0, Cc, s0, s1,
+                                s00, s11, s22, a.eta, pf[(L::NPF - 2) * NT], pf[(L::NPF - 1) * NT], ku, kv, br, ju,
+                                jv);
+      } else {
+        point_rhs<T>(q[p + 5], pf[0], pf[NT], pf[2 * NT], pf[3 * NT], C22, C00, C11, C1, C0, Cc, s0, s1, s00, s11,
+                     s22, a.eta, ku, kv, br);
+      }
       // RK combination and stores (store_point's arithmetic, 32-bit offsets)
       T accu = (STAGE == 1) ? (T)0 : pf[7 * NT];
       T accv = (STAGE == 1) ? (T)0 : pf[8 * NT];
@@ -252,14 +267,14 @@ __device__ __forceinline__ void march_block(const SubDev<T>& a, const int bid, d
     finalize_l2<T, NT>(a, sh);
 }
 
-template <typename T, int STAGE, bool RESID, int BY, int PZ, int D, int MINB>
+template <typename T, int STAGE, bool RESID, int BY, int PZ, int D, int MINB, bool CORR = false>
 __global__ void __launch_bounds__(32 * BY, MINB) k_substep_march(SubDev<T> a) {
   extern __shared__ __align__(16) double dsm[];
   __shared__ double sh[BY > 8 ? BY : 8];
   __shared__ bool last;
   pdl_enter();
   if (*a.done) return;
-  march_block<T, STAGE, RESID, BY, PZ, D, true>(a, blockIdx.x, dsm, sh, &last);
+  march_block<T, STAGE, RESID, BY, PZ, D, true, CORR>(a, blockIdx.x, dsm, sh, &last);
 }
 
 // One substep of many grids in one launch: the blocks of grid c are
@@ -288,10 +303,10 @@ __global__ void __launch_bounds__(32 * BY, MINB)
 
 // Opts the kernel into more than 48 KB of dynamic shared memory, once per
 // device.
-template <typename T, int STAGE, bool RESID, int BY, int PZ, int D, int MINB, bool BATCH = false>
+template <typename T, int STAGE, bool RESID, int BY, int PZ, int D, int MINB, bool BATCH = false, bool CORR = false>
 bool march_opt_in() {
   static unsigned long long devices = 0;
-  const size_t bytes = MarchSmem<T, BY, STAGE, D>::bytes;
+  const size_t bytes = MarchSmem<T, BY, STAGE, D, CORR>::bytes;
   if (bytes <= 48 * 1024) return true;
   int dev = 0;
   NRPYELL_CUDA(cudaGetDevice(&dev));
@@ -300,7 +315,7 @@ bool march_opt_in() {
       NRPYELL_CUDA(cudaFuncSetAttribute(k_substep_march_batch<T, STAGE, RESID, BY, PZ, D, MINB>,
                                         cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes));
     else
-      NRPYELL_CUDA(cudaFuncSetAttribute(k_substep_march<T, STAGE, RESID, BY, PZ, D, MINB>,
+      NRPYELL_CUDA(cudaFuncSetAttribute(k_substep_march<T, STAGE, RESID, BY, PZ, D, MINB, CORR>,
                                         cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes));
     devices |= 1ull << dev;
   }
@@ -378,9 +393,11 @@ MarchSplit march_split(const Dims& d, int ncol) {
   return s;
 }
 
-template <typename T, int STAGE, bool RESID, int BY, int PZ, int D, int MINB>
+// The correction form takes the plain form's split (the stop test's
+// reduction sums exactly march_interior_blocks partials).
+template <typename T, int STAGE, bool RESID, int BY, int PZ, int D, int MINB, bool CORR = false>
 void launch_march_shape(const SubstepArgs& a) {
-  if (!march_opt_in<T, STAGE, RESID, BY, PZ, D, MINB>()) return;
+  if (!march_opt_in<T, STAGE, RESID, BY, PZ, D, MINB, false, CORR>()) return;
   SubDev<T> f = make_dev<T>(a, BY, PZ);
   f.n_col_blocks = ((a.d.Nxx1 + kRows - 1) / kRows) * a.d.Nxx2;
   // the split is chosen once per grid size and shape (stage 2's occupancy)
@@ -388,8 +405,8 @@ void launch_march_shape(const SubstepArgs& a) {
   f.mbig = sp.nb;
   f.msmall = sp.small;
   f.n_tiles = f.tiles0 * f.tiles1 * (sp.nb + sp.ns);
-  NRPYELL_LAUNCH_PDL((k_substep_march<T, STAGE, RESID, BY, PZ, D, MINB>), f.n_tiles + f.n_col_blocks, 32 * BY,
-                     (MarchSmem<T, BY, STAGE, D>::bytes), f);
+  NRPYELL_LAUNCH_PDL((k_substep_march<T, STAGE, RESID, BY, PZ, D, MINB, CORR>), f.n_tiles + f.n_col_blocks, 32 * BY,
+                     (MarchSmem<T, BY, STAGE, D, CORR>::bytes), f);
 }
 
 // The compiled shapes, by index: (BY, PZ, ring slots D, minimum resident
@@ -398,12 +415,12 @@ void launch_march_shape(const SubstepArgs& a) {
   X(0, 8, 8, 3, 2) X(1, 8, 16, 2, 3) X(2, 8, 4, 2, 4) X(3, 8, 4, 2, 3) X(4, 8, 8, 2, 3) X(5, 8, 32, 2, 3) \
       X(6, 8, 4, 3, 2)
 
-template <typename T, int STAGE, bool RESID>
+template <typename T, int STAGE, bool RESID, bool CORR = false>
 bool march_stage(int v, const SubstepArgs& a) {
   switch (v) {
 #define NRPYELL_MARCH(I, BY, PZ, D, MINB)                          \
   case I:                                                          \
-    launch_march_shape<T, STAGE, RESID, BY, PZ, D, MINB>(a);       \
+    launch_march_shape<T, STAGE, RESID, BY, PZ, D, MINB, CORR>(a); \
     return true;
     NRPYELL_MARCH_SHAPES(NRPYELL_MARCH)
 #undef NRPYELL_MARCH
@@ -438,6 +455,13 @@ void opt_in_shape() {
   march_opt_in<T, 2, false, BY, PZ, D, MINB>();
   march_opt_in<T, 3, false, BY, PZ, D, MINB>();
   march_opt_in<T, 4, false, BY, PZ, D, MINB>();
+  if constexpr (sizeof(T) == 4) {
+    march_opt_in<T, 1, true, BY, PZ, D, MINB, false, true>();
+    march_opt_in<T, 1, false, BY, PZ, D, MINB, false, true>();
+    march_opt_in<T, 2, false, BY, PZ, D, MINB, false, true>();
+    march_opt_in<T, 3, false, BY, PZ, D, MINB, false, true>();
+    march_opt_in<T, 4, false, BY, PZ, D, MINB, false, true>();
+  }
 }
 
 }  // namespace
@@ -448,6 +472,18 @@ template <typename T>
 bool launch_march(int stage, bool resid, int v, const SubstepArgs& a) {
   if (!march_fits(a.d)) return false;
   bool ok = false;
+  if (a.R0) {  // the correction form (FP32 only)
+    if constexpr (sizeof(T) == 4) {
+      switch (stage) {
+        case 1: ok = resid ? march_stage<T, 1, true, true>(v, a) : march_stage<T, 1, false, true>(v, a); break;
+        case 2: ok = march_stage<T, 2, false, true>(v, a); break;
+        case 3: ok = march_stage<T, 3, false, true>(v, a); break;
+        default: ok = march_stage<T, 4, false, true>(v, a); break;
+      }
+    }
+    if (!ok) NRPYELL_FAIL("launch_march: the correction form exists for FP32 marching shapes only");
+    return true;
+  }
   switch (stage) {
     case 1: ok = resid ? march_stage<T, 1, true>(v, a) : march_stage<T, 1, false>(v, a); break;
     case 2: ok = march_stage<T, 2, false>(v, a); break;

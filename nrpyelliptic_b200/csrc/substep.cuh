@@ -30,6 +30,12 @@ struct SubDev {
   T* acc;
   T* out;
   const T* __restrict__ aux;
+  // Correction form (FP32 relaxation of a correction to an FP64 state, see
+  // point_rhs_correction): the RHS of the FP64 base state, R0[0] the uu RHS
+  // and R0[1] the residual bracket at interior points / the vv RHS at the
+  // radiation ghost points; aux then holds S(U) = ADD_times_AUU/(8 P^7),
+  // P = psi_background + U and the wavespeed.  nullptr otherwise.
+  const T* __restrict__ R0;
   const T* __restrict__ coef;
   const double* __restrict__ colgeo;
   const double* __restrict__ w;  // L2 weights (stage-1 residual)
@@ -116,6 +122,45 @@ __device__ __forceinline__ void point_rhs(T c, T vv, T AA, T psi, T ws, T C22, T
   bracket = fma((T)0.125, AA / pu7, lap);
   ku = fma(-eta, c, vv);
   kv = (ws * ws) * bracket;
+}
+
+// Correction form of point_rhs.  The state is U + d with U an FP64 base state
+// that stays fixed over a stretch of steps and d = (c, vv) the correction the
+// kernel relaxes (in FP32).  The RHS is affine in the state except for the
+// puncture source S(u) = ADD_times_AUU / (8 (psi + u)^7), so
+//   uu RHS  = R0u + (vv - eta c)
+//   bracket = R0b + lap(c) + [S(U + c) - S(U)]
+//   vv RHS  = ws^2 * bracket,
+// with R0u = V - eta U and R0b = lap(U) + S(U) evaluated in FP64.  The source
+// difference is written as
+//   S(U + c) - S(U) = -S(U) (c / (P + c)) (1 + r + ... + r^6),  r = P / (P + c),
+// P = psi + U, so every term carries its own relative rounding error and
+// the FP32 error of the whole RHS scales with the correction, not with U.
+// ju and jv return the correction parts (vv - eta c, ws^2 (lap + dS)): the
+// radiation BC, linear in the state, takes them as its interior input.
+template <typename T>
+__device__ __forceinline__ void point_rhs_correction(T c, T vv, T S, T P, T ws, T C22, T C00, T C11, T C1, T C0, T Cc,
+                                                     T s0, T s1, T s00, T s11, T s22, T eta, T R0u, T R0b, T& ku,
+                                                     T& kv, T& bracket, T& ju, T& jv) {
+  T lap = Cc * c;
+  lap = fma(C00, s00, lap);
+  lap = fma(C11, s11, lap);
+  lap = fma(C22, s22, lap);
+  lap = fma(C1, s1, lap);
+  lap = fma(C0, s0, lap);
+  const T q = (T)1 / (P + c);
+  const T r = P * q;
+  T sum = fma(r, (T)1, (T)1);
+#pragma unroll
+  for (int k = 0; k < 5; k++) sum = fma(r, sum, (T)1);
+  const T dS = -S * (c * q) * sum;
+  const T jb = lap + dS;
+  const T w2 = ws * ws;
+  bracket = R0b + jb;
+  ju = fma(-eta, c, vv);
+  ku = R0u + ju;
+  kv = w2 * bracket;
+  jv = w2 * jb;
 }
 
 // Loads the pointwise values at idx / k2 and evaluates point_rhs.
@@ -406,19 +451,29 @@ constexpr int kRows = 32;
 // [kRows][2][6], kl [kRows][2], kk [kRows][2][5], and G[kRows][kColG]: per
 // column the values the RHS of its last interior point reads outside F
 // (uu at i2 +- 1..5, vv, the three auxevol fields, the six metric weights).
+// The correction form (CORR) adds R0u and R0b of the last interior point
+// (items 20, 21).
 constexpr int kColG = 20;
 constexpr int kRowsSmem = 2 * (kRows + 10) * 12 + 2 * kRows * 12 + kRows * 2 + kRows * 10 + kRows * kColG;
+constexpr int kColGCorr = 22;
+constexpr int kRowsSmemCorr = kRowsSmem + kRows * (kColGCorr - kColG);
 
-template <typename T, int STAGE, int NT>
+// CORR: the correction form (point_rhs_correction).  The radiation BC is
+// linear in the state and in the interior RHS it starts from, so the layers
+// are computed from the correction alone (its radial derivatives and the
+// correction part of the last interior point's RHS) and the base state's
+// RHS at the ghost point, R0, is added before the RK combination.
+template <typename T, int STAGE, int NT, bool CORR = false>
 __device__ void column_rows(const SubDev<T>& a, int cb, double* smem) {
   static_assert(NT >= 2 * kRows, "the layer recurrence takes one thread per column and gridfunction");
+  constexpr int NCG = CORR ? kColGCorr : kColG;
   constexpr int NRW = kRows + 10, NQ = 12;
   double(*F)[NRW][NQ] = reinterpret_cast<double(*)[NRW][NQ]>(smem);
   double(*drf)[2][6] = reinterpret_cast<double(*)[2][6]>(smem + 2 * NRW * NQ);
   double(*fvs)[2][6] = reinterpret_cast<double(*)[2][6]>(smem + 2 * NRW * NQ + kRows * 12);
   double(*kl)[2] = reinterpret_cast<double(*)[2]>(smem + 2 * NRW * NQ + 2 * kRows * 12);
   double(*kk)[2][5] = reinterpret_cast<double(*)[2][5]>(smem + 2 * NRW * NQ + 2 * kRows * 12 + 2 * kRows);
-  double(*G)[kColG] = reinterpret_cast<double(*)[kColG]>(smem + 2 * NRW * NQ + 2 * kRows * 12 + 2 * kRows + 10 * kRows);
+  double(*G)[NCG] = reinterpret_cast<double(*)[NCG]>(smem + 2 * NRW * NQ + 2 * kRows * 12 + 2 * kRows + 10 * kRows);
   const int tid = threadIdx.x;
   const int nb1 = (a.Nxx1 + kRows - 1) / kRows;
   const int i1a = NGHOSTS + (cb % nb1) * kRows;
@@ -442,9 +497,9 @@ __device__ void column_rows(const SubDev<T>& a, int cb, double* smem) {
   }
   // the rest of each column's last-interior-point inputs, spread over the
   // block (item m of column c: 0..9 uu at i2 -+ 1..5, 10 vv, 11..13 auxevol,
-  // 14..19 metric weights)
-  for (int e = tid; e < kRows * kColG; e += NT) {
-    const int c = e / kColG, m = e - c * kColG;
+  // 14..19 metric weights, CORR: 20..21 R0u, R0b)
+  for (int e = tid; e < kRows * NCG; e += NT) {
+    const int c = e / NCG, m = e - c * NCG;
     if (c >= ncol) continue;
     const long long line = (N0 - NGHOSTS - 1) + (long long)N0 * (i1a + c);
     const T* src;
@@ -456,8 +511,10 @@ __device__ void column_rows(const SubDev<T>& a, int cb, double* smem) {
     } else if (m < 14) {
       const int gf = m == 11 ? ADD_TIMES_AUUGF : (m == 12 ? PSI_BACKGROUNDGF : WAVESPEEDGF);
       src = a.aux + gf * a.Ntot + line + a.N01 * i2;
-    } else {
+    } else if (m < 20) {
       src = a.coef + (m - 14) * a.N01 + line;
+    } else {
+      src = a.R0 + (m - 20) * a.Ntot + line + a.N01 * i2;
     }
     G[c][m] = (double)__ldg(src);
   }
@@ -498,10 +555,19 @@ __device__ void column_rows(const SubDev<T>& a, int cb, double* smem) {
 #pragma unroll
       for (int k = 1; k <= 5; k++) s22 = fma(W<T>::e(k), (T)gc[2 * k - 1] + (T)gc[2 * k - 2], s22);
       T ku, kv, br;
-      point_rhs<T>((T)row[6], (T)gc[10], (T)gc[11], (T)gc[12], (T)gc[13], (T)gc[14], (T)gc[15], (T)gc[16],
-                   (T)gc[17], (T)gc[18], (T)gc[19], s0, s1, s00, s11, s22, a.eta, ku, kv, br);
-      kl[c][0] = (double)ku;
-      kl[c][1] = (double)kv;
+      if (CORR) {
+        T ju, jv;
+        point_rhs_correction<T>((T)row[6], (T)gc[10], (T)gc[11], (T)gc[12], (T)gc[13], (T)gc[14], (T)gc[15],
+                                (T)gc[16], (T)gc[17], (T)gc[18], (T)gc[19], s0, s1, s00, s11, s22, a.eta,
+                                (T)gc[NCG - 2], (T)gc[NCG - 1], ku, kv, br, ju, jv);
+        kl[c][0] = (double)ju;
+        kl[c][1] = (double)jv;
+      } else {
+        point_rhs<T>((T)row[6], (T)gc[10], (T)gc[11], (T)gc[12], (T)gc[13], (T)gc[14], (T)gc[15], (T)gc[16],
+                     (T)gc[17], (T)gc[18], (T)gc[19], s0, s1, s00, s11, s22, a.eta, ku, kv, br);
+        kl[c][0] = (double)ku;
+        kl[c][1] = (double)kv;
+      }
     }
   }
   __syncthreads();
@@ -515,7 +581,8 @@ __device__ void column_rows(const SubDev<T>& a, int cb, double* smem) {
     const long long idx = g * a.Ntot + (long long)N0 * (i1a + c) + a.N01 * i2 + N0 - NGHOSTS + L;
     T accv = (STAGE == 1) ? (T)0 : a.acc[idx];
     T ov;
-    rk_combine<T, STAGE>((T)kk[c][g][L], a.y[idx], accv, ov, a.dt);
+    const double kfull = CORR ? kk[c][g][L] + (double)__ldg(a.R0 + idx) : kk[c][g][L];
+    rk_combine<T, STAGE>((T)kfull, a.y[idx], accv, ov, a.dt);
     if (STAGE != 4) a.acc[idx] = accv;
     a.out[idx] = ov;
   }
@@ -571,6 +638,7 @@ inline SubDev<T> make_dev(const SubstepArgs& a, int by, int p) {
   f.acc = (T*)a.acc;
   f.out = (T*)a.out;
   f.aux = (const T*)a.aux;
+  f.R0 = (const T*)a.R0;
   f.coef = sizeof(T) == 8 ? (const T*)a.rt->coef : (const T*)a.rt->coef32;
   f.colgeo = a.bt->colgeo;
   f.w = a.lt ? a.lt->w : nullptr;

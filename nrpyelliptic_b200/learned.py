@@ -156,7 +156,7 @@ def timed_relax(lib, prob, ds, mixed, max_steps=40000):
     t0 = time.perf_counter()
     if mixed:
         n32, n64 = C.c_int(0), C.c_int(0)
-        lib.nrpyell_relax_mixed(C.byref(ds.g), prob.dt, -10.0, -6.0, 200, 0.98, max_steps, prob.cfg.R_L2,
+        lib.nrpyell_relax_mixed(C.byref(ds.g), prob.dt, -10.0, -10.0, 256, max_steps, prob.cfg.R_L2,
                                 C.byref(n32), C.byref(n64), C.byref(fin), None)
         steps = n32.value + n64.value
     else:

@@ -169,6 +169,18 @@ class Problem:
             out[name] = np.ctypeslib.as_array(getattr(self.rfm, name), shape=(n,)).copy()
         return out
 
+    def radius(self):
+        """r(xx0, xx1) of the SinhSymTP grid at the interior (i1, i0) points
+        (the radius L2_norm_of_gf.c:19-28 compares with the integration
+        radius), shape (Nxx1, Nxx0)."""
+        p = self.params
+        x0, x1 = self.xx_arrays()[:2]
+        x0 = x0[abi.NGHOSTS:-abi.NGHOSTS]
+        x1 = x1[abi.NGHOSTS:-abi.NGHOSTS]
+        A = p.AMAX * np.sinh(x0 / p.SINHWAA) / np.sinh(1.0 / p.SINHWAA)
+        s, c = np.sin(x1)[:, None], np.cos(x1)[:, None]
+        return np.sqrt(A[None, :] ** 2 * s ** 2 + (p.bScale ** 2 + A[None, :] ** 2) * c ** 2)
+
     def zero_state(self):
         return np.zeros(abi.NUM_EVOL_GFS * self.Ntot)
 

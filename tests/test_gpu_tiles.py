@@ -98,23 +98,23 @@ def test_every_tile_relaxes_to_the_same_solution(lib):
         lib.nrpyell_set_tile(-1)
 
 
-def test_shared_memory_tiles_in_mixed_precision(lib):
-    """The FP32 phase on the shared-memory shapes (the TMA shapes run their
-    FP32 substitute there)."""
+def test_marching_tiles_in_mixed_precision(lib):
+    """The FP32 correction form of the mixed-precision driver on every
+    marching shape (the only kind that runs it)."""
     gold = load_golden("relax_shipped_64x64x8.npz")
     prob = Problem(CONFIGS["shipped_64x64x8"])
     N = prob.N
     ref = gold["uu_interior"]
     try:
         for t, by, p, kind in tiles(lib):
-            if kind not in (3, 4, 5):
+            if kind != 5:
                 continue
             lib.nrpyell_set_tile(t)
             ds = DeviceState(prob)
             n32, n64 = C.c_int(0), C.c_int(0)
             fin = C.c_double(0)
             hist = np.zeros(6001)
-            rc = lib.nrpyell_relax_mixed(C.byref(ds.g), prob.dt, -10.0, -6.0, 200, 0.98, 6000, 100.0, C.byref(n32),
+            rc = lib.nrpyell_relax_mixed(C.byref(ds.g), prob.dt, -10.0, -10.0, 64, 6000, 100.0, C.byref(n32),
                                          C.byref(n64), C.byref(fin), ptr(hist))
             _lib.check(lib)
             assert rc == 0 and fin.value <= -10.0 and n32.value > 0, t
