@@ -309,6 +309,12 @@ int nrpyell_event_record(int slot);
 float nrpyell_event_elapsed_ms(int a, int b);
 /* Writes a 256 MiB device buffer, evicting the 126 MB L2 (benchmark hygiene). */
 void nrpyell_flush_l2(void);
+/* Copy bandwidth of the GPU in GB/s (bytes read + written per second): a
+ * 16-byte-vector copy kernel between two buffers of bytes/2 each, repeated
+ * within one launch until about 1 GiB has moved, best of `iters` timed
+ * launches after a warm-up.  A footprint below the L2 size measures L2
+ * bandwidth, a larger one HBM bandwidth.  Allocates and frees its buffers. */
+double nrpyell_copy_bandwidth(size_t bytes, int iters);
 /* Device time of the fused RK4 pieces on griddata's buffers, averaged over
  * n_iter launches replayed from a CUDA graph (the buffers are modified):
  *   ms_interior: one fused interior kernel of RK4 stage `stage` (1..4)

@@ -40,6 +40,7 @@ EXPORTS = {
     "nrpyell_abi_layout": (C.c_int, [P(C.c_int), C.c_int]),
     "nrpyell_launch_count": (C.c_longlong, []),
     "nrpyell_device_alloc_count": (C.c_longlong, []),
+    "nrpyell_copy_bandwidth": (C.c_double, [C.c_size_t, C.c_int]),
     "nrpyell_set_step_mode": (None, [C.c_int]),
     "nrpyell_get_step_mode": (C.c_int, []),
     "nrpyell_set_device": (C.c_int, [C.c_int]),

@@ -177,6 +177,15 @@ struct RelaxSetup {
   Scratch* s;
 };
 
+// Copy kernel of nrpyell_copy_bandwidth: 16-byte loads and stores, grid-stride.
+// `passes` sweeps over the same buffers in one launch, so that a footprint
+// that fits in L2 is measured without the launch latency.
+__global__ void k_copy_bw(const double2* __restrict__ a, double2* __restrict__ b, long long n, int passes) {
+  for (int p = 0; p < passes; p++)
+    for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
+      b[i] = a[i];
+}
+
 // Longest FP32 stretch of nrpyell_relax_mixed between two folds.
 constexpr int kMaxFoldEvery = 4096;
 
@@ -304,6 +313,44 @@ float nrpyell_event_elapsed_ms(int a, int b) {
   NRPYELL_CUDA(cudaEventSynchronize(g_events[b]));
   NRPYELL_CUDA(cudaEventElapsedTime(&ms, g_events[a], g_events[b]));
   return ms;
+}
+
+double nrpyell_copy_bandwidth(size_t bytes, int iters) {
+  const long long n = (long long)(bytes / 2 / sizeof(double2));
+  if (n < 1 || iters < 1) {
+    NRPYELL_FAIL("nrpyell_copy_bandwidth: need bytes >= 32 and iters >= 1");
+    return -1.0;
+  }
+  double2 *a = nullptr, *b = nullptr;
+  NRPYELL_CUDA(dev_alloc(&a, sizeof(double2) * n));
+  NRPYELL_CUDA(dev_alloc(&b, sizeof(double2) * n));
+  cudaEvent_t e0, e1;
+  NRPYELL_CUDA(cudaEventCreate(&e0));
+  NRPYELL_CUDA(cudaEventCreate(&e1));
+  if (!status_ok()) return -1.0;
+  NRPYELL_CUDA(cudaMemsetAsync(a, 0, sizeof(double2) * n, stream()));
+  int sms = 148;
+  int dev = 0;
+  NRPYELL_CUDA(cudaGetDevice(&dev));
+  NRPYELL_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+  const unsigned grid = (unsigned)std::min<long long>((n + 255) / 256, (long long)sms * 8);
+  const int passes = (int)std::max<long long>(1, (1ll << 30) / (long long)(2 * sizeof(double2) * n));
+  float best = 1e30f;
+  for (int it = 0; it <= iters; it++) {  // the first launch is a warm-up
+    NRPYELL_CUDA(cudaEventRecord(e0, stream()));
+    NRPYELL_LAUNCH(k_copy_bw, grid, 256, 0, a, b, n, passes);
+    NRPYELL_CUDA(cudaEventRecord(e1, stream()));
+    NRPYELL_CUDA(cudaEventSynchronize(e1));
+    float ms = 0.0f;
+    NRPYELL_CUDA(cudaEventElapsedTime(&ms, e0, e1));
+    if (it > 0) best = std::min(best, ms);
+  }
+  NRPYELL_CUDA(cudaEventDestroy(e0));
+  NRPYELL_CUDA(cudaEventDestroy(e1));
+  NRPYELL_CUDA(cudaFree(a));
+  NRPYELL_CUDA(cudaFree(b));
+  if (!status_ok()) return -1.0;
+  return 2.0 * sizeof(double2) * n * passes / (best * 1e-3) / 1e9;
 }
 
 void nrpyell_flush_l2(void) {

@@ -109,6 +109,7 @@ class Guess:
         x = self._upload((feats - self.fmu) / self.fsd)
         t = self._upload(coeffs / self.csd)
         hist = np.zeros(epochs)
+        batch = min(batch, len(feats))
         last = self.lib.nrpyell_mlp_train(self.mlp, x, t, len(feats), batch, epochs, lr, seed, hist.ctypes.data)
         _lib.check(self.lib)
         self.lib.nrpyell_device_free(x)
@@ -149,6 +150,22 @@ def initial_log10_l2(lib, prob, ds):
     return fin.value
 
 
+def start_state(lib, prob, ds, guess, coeffs, r0=None):
+    """Puts the learned guess for one configuration into ds's y_n and keeps it
+    only if its residual L2 is below the zero guess's (r0, evaluated here
+    when None); otherwise ds gets the zero guess (the fallback).  Returns
+    (learned guess used, log10 L2 of the zero guess, of the learned guess)."""
+    if r0 is None:
+        ds.set_state(prob.zero_state())
+        r0 = initial_log10_l2(lib, prob, ds)
+    guess.write_guess(coeffs, prob.cfg.eta, C.c_void_p(ds.ptr["y_n"]))
+    rl = initial_log10_l2(lib, prob, ds)
+    use = bool(rl < r0)
+    if not use:
+        ds.set_state(prob.zero_state())
+    return use, r0, rl
+
+
 def timed_relax(lib, prob, ds, mixed, max_steps=40000):
     """(RK4 steps, seconds, final log10 L2) of one relaxation from ds's state."""
     fin = C.c_double(0)
@@ -187,10 +204,8 @@ def evaluate(lib, guess, cfgs, log=print):
         u_zero = ds.download("y_n", prob.Ntot)
         guess.write_guess(coeffs[i], cfg.eta, C.c_void_p(ds.ptr["y_n"]))
         u_guess = ds.download("y_n", prob.Ntot)
-        rl = initial_log10_l2(lib, prob, ds)
-        fallback = not (rl < r0)
-        if fallback:
-            ds.set_state(prob.zero_state())
+        use, _, rl = start_state(lib, prob, ds, guess, coeffs[i], r0)
+        fallback = not use
         s1, t1, f1 = timed_relax(lib, prob, ds, False)
         u_learned = ds.download("y_n", prob.Ntot)
         if fallback:
@@ -212,6 +227,68 @@ def evaluate(lib, guess, cfgs, log=print):
     a = np.array(rows, dtype=np.float64)
     out = {k: a[:, j] for j, k in enumerate(KEYS)}
     out["u_zero"] = zeros  # converged solutions from the zero guess
+    return out
+
+
+def compare_solvers(lib, guess, cfgs, log=print):
+    """Wall time of the held-out configurations solved (a) one by one in FP64
+    from the zero guess -- the plain form -- and from the learned guess with
+    the fallback rule (b) one by one in FP64, (c) one by one with the FP32
+    correction form of the mixed-precision driver, (d) all together in one
+    batched FP64 relaxation.  Set-up (grids, tables, auxevol) is outside the
+    timings; the learned guess's network evaluation, guess writing and
+    fallback test are inside (b)-(d).  Returns a dict of solves/s, RK4 steps
+    and the speed-up of each form over (a)."""
+    from .batch import relax_batch
+    probs = [Problem(c, lib=lib, host_aux=False) for c in cfgs]
+    states = [DeviceState(p, lib=lib) for p in probs]
+    n = len(cfgs)
+    out = {"configurations": n}
+
+    def clock(fn):
+        lib.nrpyell_synchronize()
+        t0 = time.perf_counter()
+        r = fn()
+        lib.nrpyell_synchronize()
+        return time.perf_counter() - t0, r
+
+    # warm-up: tile tuning, and the graph capture of both drivers for every
+    # configuration's buffers (graphs are cached per buffers)
+    for p, ds in zip(probs, states):
+        initial_log10_l2(lib, p, ds)
+        timed_relax(lib, p, ds, False, max_steps=32)
+        timed_relax(lib, p, ds, True, max_steps=600)
+    relax_batch(probs, states, max_steps=32, lib=lib)
+    for p, ds in zip(probs, states):
+        ds.set_state(p.zero_state())
+    t, steps = clock(lambda: [timed_relax(lib, p, ds, False)[0] for p, ds in zip(probs, states)])
+    out["fp64_zero_guess"] = {"solves_per_s": n / t, "steps_median": float(np.median(steps))}
+
+    def learned_starts():
+        coeffs = guess.predict([features(c) for c in cfgs])
+        return [start_state(lib, p, ds, guess, coeffs[i])[0] for i, (p, ds) in enumerate(zip(probs, states))]
+
+    def single(mixed):
+        used = learned_starts()
+        return used, [timed_relax(lib, p, ds, mixed)[0] for p, ds in zip(probs, states)]
+
+    for key, mixed in (("fp64_learned", False), ("mixed_learned", True)):
+        t, (used, steps) = clock(lambda: single(mixed))
+        out[key] = {"solves_per_s": n / t, "steps_median": float(np.median(steps)), "fallbacks": n - int(sum(used))}
+
+    def batched():
+        used = learned_starts()
+        rc, steps, _, _ = relax_batch(probs, states, lib=lib)
+        return used, steps, rc
+    t, (used, steps, rc) = clock(batched)
+    out["batched_fp64_learned"] = {"solves_per_s": n / t, "steps_median": float(np.median(steps)),
+                                   "fallbacks": n - int(sum(used)), "not_converged": int(rc)}
+    base = out["fp64_zero_guess"]["solves_per_s"]
+    for k in ("fp64_learned", "mixed_learned", "batched_fp64_learned"):
+        out[k]["speedup_vs_fp64_zero_guess"] = out[k]["solves_per_s"] / base
+    for ds in states:
+        ds.free()
+    lib.nrpyell_release_tables()
     return out
 
 

@@ -1,0 +1,98 @@
+"""The learned initial guess end to end on a small grid (32x32x8, the
+seeded sweep distribution): batched training solves, POD, MLP training with
+the library's BF16 tensor-core kernels, the POD guess kernel, the fallback
+rule and the relaxation from the learned start.
+
+Checks:
+  * k_pod_guess writes uu = mean + sum_k c_k basis_k and vv = eta uu
+    (relative 1e-6: float32 basis, float64 sum);
+  * the fallback rule keeps the learned guess exactly where its residual
+    L2 is below the zero guess's, and rejects a deliberately wrong guess;
+  * on held-out draws the learned start takes fewer RK4 steps (median) than
+    the zero guess, and every relaxation reaches log10 L2 <= -10 with a
+    solution within 1e-6 of max|uu| of the zero-guess solution: two
+    solutions at that residual reached along different paths (the stop
+    test's norm covers r < R_L2 only; measured 1.5e-7 on this grid).
+"""
+import ctypes as C
+
+import numpy as np
+import pytest
+
+from nrpyelliptic_b200 import _lib
+from nrpyelliptic_b200.learned import Guess, evaluate, features, pod, solve_snapshots, start_state
+from nrpyelliptic_b200.problem import DeviceState, Problem, sample_sweep, with_grid
+
+pytestmark = pytest.mark.gpu
+GRID = (32, 32, 8)
+
+
+def draws(n, seed):
+    return [with_grid(c, GRID) for c in sample_sweep(n, seed)]
+
+
+@pytest.fixture(scope="module")
+def trained():
+    lib = _lib.load()
+    lib.nrpyell_clear_status()
+    cfgs = draws(384, 7001)
+    snaps, steps = solve_snapshots(cfgs, lib, chunk=128, log=lambda *a: None)
+    assert np.all(steps > 0)
+    mean, basis, coeffs, energy = pod(snaps, 24)
+    feats = np.array([features(c) for c in cfgs])
+    guess = Guess(lib, mean, basis, coeffs, feats)
+    last, hist = guess.train(feats, coeffs, 300)
+    yield lib, guess, mean, basis, coeffs, hist, energy
+    guess.free()
+
+
+def test_training_lowers_the_loss(trained):
+    lib, guess, mean, basis, coeffs, hist, energy = trained
+    assert energy > 0.999
+    assert hist[-1] < 0.05 * hist[0], (hist[0], hist[-1])
+
+
+def test_pod_guess_kernel_writes_the_reconstruction(trained):
+    lib, guess, mean, basis, coeffs, hist, energy = trained
+    prob = Problem(draws(1, 9)[0], lib=lib, host_aux=False)
+    ds = DeviceState(prob, lib=lib)
+    c = coeffs[3]
+    guess.write_guess(c, prob.cfg.eta, C.c_void_p(ds.ptr["y_n"]))
+    y = ds.download("y_n")
+    uu = mean.astype(np.float64) + c.astype(np.float32).astype(np.float64) @ basis.astype(np.float64)
+    n = prob.Ntot
+    assert np.max(np.abs(y[:n] - uu)) <= 1e-6 * np.max(np.abs(uu))
+    np.testing.assert_allclose(y[n:], prob.cfg.eta * y[:n], rtol=1e-15, atol=0)
+    ds.free()
+
+
+def test_fallback_rejects_a_wrong_guess(trained):
+    lib, guess, mean, basis, coeffs, hist, energy = trained
+    prob = Problem(draws(1, 11)[0], lib=lib, host_aux=False)
+    ds = DeviceState(prob, lib=lib)
+    good = guess.predict([features(prob.cfg)])[0]
+    use, r0, rl = start_state(lib, prob, ds, guess, good)
+    assert use == (rl < r0)
+    # a guess 50x too large: its residual is far above the zero guess's
+    use, r0, rl = start_state(lib, prob, ds, guess, 50.0 * good)
+    assert not use and rl > r0
+    assert not np.any(ds.download("y_n"))  # the zero guess is in place
+    ds.free()
+
+
+def test_learned_guess_saves_steps_on_held_out_draws(trained):
+    lib, guess, mean, basis, coeffs, hist, energy = trained
+    ev = evaluate(lib, guess, draws(24, 7002), log=lambda *a: None)
+    ev.pop("u_zero")
+    fb = ev["fallback"].astype(bool)
+    np.testing.assert_array_equal(fb, ~(ev["res_learned"] < ev["res0"]))
+    saved = 1.0 - ev["steps_learned"] / ev["steps_zero"]
+    print("learned guess 32x32x8: fallbacks %d / %d, guess rel L2 error median %.2e, steps zero %d -> learned %d "
+          "(median saving %.1f %%), max |uu - uu_zero| / max|uu|: learned %.2e, learned + mixed %.2e"
+          % (fb.sum(), len(fb), np.median(ev["guess_rel_l2"]), np.median(ev["steps_zero"]),
+             np.median(ev["steps_learned"]), 100 * np.median(saved), ev["err_learned"].max(), ev["err_mixed"].max()))
+    for k in ("fin_zero", "fin_learned", "fin_mixed"):
+        assert ev[k].max() <= -10.0, k
+    assert ev["err_learned"].max() <= 1e-6 and ev["err_mixed"].max() <= 1e-6
+    assert fb.sum() <= len(fb) // 2
+    assert np.median(ev["steps_learned"]) < np.median(ev["steps_zero"])
