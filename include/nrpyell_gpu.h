@@ -260,6 +260,21 @@ void nrpyell_set_optimum_eta_damping(const REAL dt, const REAL CFL_FACTOR, param
  * order xx xy xz yy yz zz. */
 int nrpyell_interpolate_solution(const paramstruct *params, REAL *xx[3], const REAL *uu, int npts, const REAL *xyz,
                                  int order, REAL *uu_out, REAL *psi_out, REAL *gamma_out, REAL *K_out);
+/* Initial lapse at npts Cartesian points (host arrays), the thorn's
+ * initial_lapse options (conformally_flat_BBH_compute_ADM_Cartesian_quantities_from_uu.c:25-29):
+ *  NRPYELL_LAPSE_PSI_POWER ("NRPyEllipticET-psi^n",
+ *    conformally_flat_BBH_lapse_power_of_psi_initial_data.c):
+ *    alpha = (1 + m0/(2 r0) + m1/(2 r1) + uu)^lapse_exponent, uu_at_points
+ *    from nrpyell_interpolate_solution (the thorn's default exponent is -2);
+ *  NRPYELL_LAPSE_AVERAGED ("NRPyEllipticET-averaged",
+ *    conformally_flat_BBH_lapse_averaged_initial_data.c):
+ *    alpha = (1 - s)/(2 (1 + s)) + 1/2 with s = m0/(2 r0) + m1/(2 r1);
+ *    uu_at_points and lapse_exponent are not used (may be NULL / 0).
+ * r_i is the distance to puncture i.  Returns 0, or -1 on bad arguments. */
+#define NRPYELL_LAPSE_PSI_POWER 0
+#define NRPYELL_LAPSE_AVERAGED 1
+int nrpyell_initial_lapse(const paramstruct *params, int npts, const REAL *xyz, const REAL *uu_at_points, int mode,
+                          REAL lapse_exponent, REAL *alpha_out);
 /* Batched relaxation: n configurations, each a griddata_struct set up as for
  * nrpyell_relax (its own grid size, parameters, bc_struct, rfm_struct and
  * device gridfunctions; dt[c] its time step), relaxed together from their

@@ -16,6 +16,8 @@
 // Lagrange molecule of order n (n+1 points per direction): for even n
 // centred on the nearest grid point, for odd n starting n/2 points below the
 // point's cell; shifted to stay inside the array.
+#include <string.h>
+
 #include "common.cuh"
 #include "sinhsymtp.h"
 
@@ -109,11 +111,64 @@ __global__ void k_export(ExportArgs a, int npts, const double* __restrict__ xyz,
   }
 }
 
+// Initial lapse at points (the thorn's two options,
+// conformally_flat_BBH_compute_ADM_Cartesian_quantities_from_uu.c:25-29):
+//   mode 0 "NRPyEllipticET-psi^n" (conformally_flat_BBH_lapse_power_of_psi_initial_data.c):
+//          alpha = (psi_BL + uu)^n, psi_BL = 1 + m0/(2 r0) + m1/(2 r1);
+//   mode 1 "NRPyEllipticET-averaged" (conformally_flat_BBH_lapse_averaged_initial_data.c):
+//          alpha = 1/2 (1 - s)/(1 + s) + 1/2, s = m0/(2 r0) + m1/(2 r1)
+//          (uu does not enter).
+__global__ void k_lapse(ExportArgs a, int npts, const double* __restrict__ xyz, const double* __restrict__ uu,
+                        int mode, double n, double* __restrict__ alpha) {
+  const int p = blockIdx.x * blockDim.x + threadIdx.x;
+  if (p >= npts) return;
+  const double X = xyz[3 * p], Y = xyz[3 * p + 1], Z = xyz[3 * p + 2];
+  const double d0x = X - a.b0.pos[0], d0y = Y - a.b0.pos[1], d0z = Z - a.b0.pos[2];
+  const double d1x = X - a.b1.pos[0], d1y = Y - a.b1.pos[1], d1z = Z - a.b1.pos[2];
+  const double s = 0.5 * a.m0 / sqrt(d0x * d0x + d0y * d0y + d0z * d0z) +
+                   0.5 * a.m1 / sqrt(d1x * d1x + d1y * d1y + d1z * d1z);
+  alpha[p] = mode == 0 ? pow(1.0 + s + uu[p], n) : 0.5 * (1.0 - s) / (1.0 + s) + 0.5;
+}
+
 }  // namespace
 
 }  // namespace nrpyell
 
 using namespace nrpyell;
+
+extern "C" int nrpyell_initial_lapse(const paramstruct* p, const int npts, const REAL* xyz, const REAL* uu_at_points,
+                                     const int mode, const REAL lapse_exponent, REAL* alpha_out) {
+  if (!p || npts < 0 || (npts > 0 && (!xyz || !alpha_out)) || (mode != NRPYELL_LAPSE_PSI_POWER &&
+                                                                mode != NRPYELL_LAPSE_AVERAGED) ||
+      (mode == NRPYELL_LAPSE_PSI_POWER && npts > 0 && !uu_at_points)) {
+    NRPYELL_FAIL("nrpyell_initial_lapse: need params, xyz, alpha_out, a known mode and uu_at_points for psi^n");
+    return -1;
+  }
+  if (npts == 0) return 0;
+  ExportArgs a;
+  memset(&a, 0, sizeof(a));
+  a.m0 = p->bare_mass_0;
+  a.m1 = p->bare_mass_1;
+  a.b0.pos[0] = p->puncture_0_x;
+  a.b0.pos[1] = p->puncture_0_y;
+  a.b0.pos[2] = p->puncture_0_z;
+  a.b1.pos[0] = p->puncture_1_x;
+  a.b1.pos[1] = p->puncture_1_y;
+  a.b1.pos[2] = p->puncture_1_z;
+  const size_t n = (size_t)npts;
+  double* buf = nullptr;
+  NRPYELL_CUDA(dev_alloc(&buf, sizeof(double) * n * 5));
+  if (!status_ok()) return -1;
+  double *d_xyz = buf, *d_uu = buf + 3 * n, *d_alpha = buf + 4 * n;
+  NRPYELL_CUDA(cudaMemcpyAsync(d_xyz, xyz, sizeof(double) * 3 * n, cudaMemcpyHostToDevice, stream()));
+  if (mode == NRPYELL_LAPSE_PSI_POWER)
+    NRPYELL_CUDA(cudaMemcpyAsync(d_uu, uu_at_points, sizeof(double) * n, cudaMemcpyHostToDevice, stream()));
+  NRPYELL_LAUNCH(k_lapse, (unsigned)((n + 127) / 128), 128, 0, a, npts, d_xyz, d_uu, mode, lapse_exponent, d_alpha);
+  NRPYELL_CUDA(cudaMemcpyAsync(alpha_out, d_alpha, sizeof(double) * n, cudaMemcpyDeviceToHost, stream()));
+  NRPYELL_CUDA(cudaStreamSynchronize(stream()));
+  cudaFree(buf);
+  return status_ok() ? 0 : -1;
+}
 
 extern "C" int nrpyell_interpolate_solution(const paramstruct* p, REAL* xx[3], const REAL* uu, const int npts,
                                             const REAL* xyz, const int order, REAL* uu_out, REAL* psi_out,

@@ -3,6 +3,7 @@ Cartesian points (nrpyell_interpolate_solution), and a binary dump of the
 uu gridfunction.
 
     uu, psi, gamma, K = interpolate(prob, ds, xyz, order=4)
+    alpha = initial_lapse(prob, xyz, uu, mode="psi^n", exponent=-2.0)
     dump_uu(prob, ds, "uu.npy")
 """
 import ctypes as C
@@ -26,6 +27,25 @@ def interpolate(prob, ds, xyz, order=4):
                                      P(gamma), P(K))
     _lib.check(lib)
     return uu, psi, gamma, K
+
+
+LAPSE_MODES = {"psi^n": 0, "averaged": 1}
+
+
+def initial_lapse(prob, xyz, uu=None, mode="psi^n", exponent=-2.0):
+    """The thorn's initial lapse at the points xyz [n x 3]: "psi^n" (alpha =
+    (psi_BL + uu)^exponent, uu at the points from interpolate()) or
+    "averaged" (from the Brill-Lindquist term alone)."""
+    lib = prob.lib
+    xyz = np.ascontiguousarray(xyz, dtype=np.float64).reshape(-1, 3)
+    n = len(xyz)
+    alpha = np.zeros(n)
+    P = lambda a: a.ctypes.data_as(abi.PREAL)
+    u = np.ascontiguousarray(uu, dtype=np.float64) if uu is not None else None
+    lib.nrpyell_initial_lapse(C.byref(prob.params), n, P(xyz), P(u) if u is not None else None, LAPSE_MODES[mode],
+                              float(exponent), P(alpha))
+    _lib.check(lib)
+    return alpha
 
 
 def dump_uu(prob, ds, path):

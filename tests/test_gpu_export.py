@@ -84,3 +84,33 @@ def test_boosted_puncture_on_its_axis(lib):
     assert np.allclose(psi, 1 + 0.5 / (2 * xs), rtol=1e-14)
     assert np.allclose(K[:, 0], 3 * 0.2 * xs / xs ** 3 / psi ** 2, rtol=1e-12)
     ds.free()
+
+
+def test_initial_lapse_options_match_their_formulas(lib):
+    """nrpyell_initial_lapse against the thorn's two formulas written out in
+    numpy (conformally_flat_BBH_lapse_power_of_psi_initial_data.c,
+    conformally_flat_BBH_lapse_averaged_initial_data.c), at random points
+    and with uu interpolated from a relaxed solution."""
+    from nrpyelliptic_b200.export import initial_lapse
+    prob = Problem(CONFIGS["shipped_64x64x8"], lib=lib)
+    ds = DeviceState(prob, lib=lib)
+    st, fin = C.c_int(0), C.c_double(0)
+    assert lib.nrpyell_relax(C.byref(ds.g), prob.dt, -10.0, 4000, 100.0, C.byref(st), C.byref(fin), None) == 0
+    p = prob.params
+    rng = np.random.default_rng(5)
+    xyz = rng.uniform(-8.0, 8.0, (200, 3))
+    uu = interpolate(prob, ds, xyz)[0]
+    r0 = np.linalg.norm(xyz - [p.puncture_0_x, p.puncture_0_y, p.puncture_0_z], axis=1)
+    r1 = np.linalg.norm(xyz - [p.puncture_1_x, p.puncture_1_y, p.puncture_1_z], axis=1)
+    s = 0.5 * p.bare_mass_0 / r0 + 0.5 * p.bare_mass_1 / r1
+    for n in (-2.0, 1.5):
+        a = initial_lapse(prob, xyz, uu, mode="psi^n", exponent=n)
+        np.testing.assert_allclose(a, (1.0 + s + uu) ** n, rtol=1e-13)
+    a = initial_lapse(prob, xyz, mode="averaged")
+    np.testing.assert_allclose(a, 0.5 * (1.0 - s) / (1.0 + s) + 0.5, rtol=1e-14)
+    # an unknown mode is an error
+    out = np.zeros(1)
+    P = lambda v: v.ctypes.data_as(C.POINTER(C.c_double))
+    assert lib.nrpyell_initial_lapse(C.byref(p), 1, P(xyz[:1].copy()), P(uu[:1].copy()), 7, 0.0, P(out)) == -1
+    lib.nrpyell_clear_status()
+    ds.free()
