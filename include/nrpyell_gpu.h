@@ -248,6 +248,27 @@ int nrpyell_relax_et(griddata_struct *griddata, const REAL dt, const REAL log_ta
  * SINHWAA = 0.07 and bScale = 5; writes params->eta_damping. */
 REAL nrpyell_compute_TRC(const REAL A, const REAL b, const REAL C_0, const REAL dt, const REAL dxx1, const REAL dxx2);
 void nrpyell_set_optimum_eta_damping(const REAL dt, const REAL CFL_FACTOR, paramstruct *params);
+/* Device tables of a grid built on the GPU (the batch set-up path): the
+ * reference-metric arrays and folded RHS weights, the inner-boundary map
+ * (SymTP images, parity +1) and the pure outer points of the x0max face with
+ * their radiation geometry -- the roles of rfm_precompute_rfmstruct_define.c:5-93
+ * and bcstruct_set_up.c:350-521 -- from params and xx alone.  rfm and bc
+ * are the structs the caller will pass to the drivers (griddata->rfmstruct,
+ * ->bcstruct); they are not read, only used as cache keys, and may be left
+ * zeroed (no host arrays).  Call after the grid is set up and before any
+ * driver, with the same params and xx.  Requires Nxx2 even and >= NGHOSTS,
+ * Nxx0 >= 12, radiation outer BCs.  Returns 0 or -1. */
+int nrpyell_setup_tables_device(const paramstruct *params, REAL *xx[3], const rfm_struct *rfm, const bc_struct *bc);
+/* Copies one device table of a grid to host memory (built from the host
+ * structs first if it does not exist): what = 0 inner map (dst, src) int32
+ * pairs, 1 inner parity int8, 2 pure outer points as 8 int32 (which_gz, dirn,
+ * i0, i1, i2, FACEX0, FACEX1, FACEX2, in the reference's list order), 3 their
+ * geometry as 6 doubles (r, dxx0/dr, dxx1/dr at the point and at its interior
+ * neighbour), 4 column geometry [3][6][N1], 5..13 f0, f0', f0'', f3, f3', f1,
+ * f1', f2, d f2/d xx0, 14 folded RHS weights [6][N0 N1].  capacity in
+ * elements; returns the number of elements written, -1 on error. */
+long long nrpyell_device_tables_read(const paramstruct *params, REAL *xx[3], const rfm_struct *rfm,
+                                     const bc_struct *bc, int what, void *host_out, long long capacity);
 /* Solution export (the Einstein Toolkit thorn's Initialize_ADMBase role,
  * without Cactus): for npts Cartesian points xyz (host, x y z per point, in
  * this code's frame), uu by Lagrange interpolation of the given order (1..8;

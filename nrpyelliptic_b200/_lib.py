@@ -85,6 +85,9 @@ EXPORTS = {
                                    P(C.c_int), P(C.c_double)]),
     "nrpyell_compute_TRC": (C.c_double, [C.c_double] * 6),
     "nrpyell_set_optimum_eta_damping": (None, [C.c_double, C.c_double, P(abi.paramstruct)]),
+    "nrpyell_setup_tables_device": (C.c_int, [P(abi.paramstruct), XX, P(abi.rfm_struct), P(abi.bc_struct)]),
+    "nrpyell_device_tables_read": (C.c_longlong, [P(abi.paramstruct), XX, P(abi.rfm_struct), P(abi.bc_struct), C.c_int,
+                                                  C.c_void_p, C.c_longlong]),
     "nrpyell_initial_lapse": (C.c_int, [P(abi.paramstruct), C.c_int, PREAL, PREAL, C.c_int, C.c_double, PREAL]),
     "nrpyell_interpolate_solution": (C.c_int, [P(abi.paramstruct), XX, PREAL, C.c_int, PREAL, C.c_int, PREAL, PREAL,
                                                PREAL, PREAL]),

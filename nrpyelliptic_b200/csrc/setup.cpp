@@ -121,24 +121,16 @@ void nrpyell_rfm_precompute_rfmstruct_freemem(const paramstruct *p, rfm_struct *
 void nrpyell_rfm_precompute_rfmstruct_define(const paramstruct *p, REAL *xx[3], rfm_struct *r) {
   const REAL AMAX = p->AMAX, SINHWAA = p->SINHWAA, bScale = p->bScale;
   const int N0 = p->Nxx_plus_2NGHOSTS0, N1 = p->Nxx_plus_2NGHOSTS1;
-  const REAL D = exp(1.0 / SINHWAA) - exp(-1 / SINHWAA);
   for (int i0 = 0; i0 < N0; i0++) {
-    const REAL x = xx[0][i0];
-    const REAL ep = exp(x / SINHWAA), em = exp(-x / SINHWAA);
-    r->f0_of_xx0[i0] = AMAX * (ep - em) / D;
-    r->f0_of_xx0__D0[i0] = AMAX * (ep / SINHWAA + em / SINHWAA) / D;
-    r->f0_of_xx0__DD00[i0] = AMAX * (ep / pow(SINHWAA, 2) - em / pow(SINHWAA, 2)) / D;
-    r->f0_of_xx0__DDD000[i0] = AMAX * (ep / pow(SINHWAA, 3) + em / pow(SINHWAA, 3)) / D;
-    const REAL A2 = pow(AMAX, 2) * pow(ep - em, 2) / pow(D, 2);
-    const REAL f3 = sqrt(A2 + pow(bScale, 2));
-    const REAL dA2 = (1.0 / 2.0) * pow(AMAX, 2) * (2 * ep / SINHWAA + 2 * em / SINHWAA) * (ep - em);  // (A^2)'/2 * D^2
-    r->f3_of_xx0[i0] = f3;
-    r->f3_of_xx0__D0[i0] = dA2 / (f3 * pow(D, 2));
-    r->f3_of_xx0__DD00[i0] =
-        -1.0 / 4.0 * pow(AMAX, 4) * pow(2 * ep / SINHWAA + 2 * em / SINHWAA, 2) * pow(ep - em, 2) /
-            (pow(A2 + pow(bScale, 2), 3.0 / 2.0) * pow(D, 4)) +
-        (1.0 / 2.0) * pow(AMAX, 2) * (2 * ep / pow(SINHWAA, 2) - 2 * em / pow(SINHWAA, 2)) * (ep - em) / (f3 * pow(D, 2)) +
-        (1.0 / 2.0) * pow(AMAX, 2) * (ep / SINHWAA + em / SINHWAA) * (2 * ep / SINHWAA + 2 * em / SINHWAA) / (f3 * pow(D, 2));
+    double o[7];
+    symtp_rfm_xx0(AMAX, SINHWAA, bScale, xx[0][i0], o);
+    r->f0_of_xx0[i0] = o[0];
+    r->f0_of_xx0__D0[i0] = o[1];
+    r->f0_of_xx0__DD00[i0] = o[2];
+    r->f0_of_xx0__DDD000[i0] = o[3];
+    r->f3_of_xx0[i0] = o[4];
+    r->f3_of_xx0__D0[i0] = o[5];
+    r->f3_of_xx0__DD00[i0] = o[6];
   }
   for (int i1 = 0; i1 < N1; i1++) {
     const REAL y = xx[1][i1];
@@ -146,29 +138,17 @@ void nrpyell_rfm_precompute_rfmstruct_define(const paramstruct *p, REAL *xx[3], 
     r->f1_of_xx1__D1[i1] = cos(y);
     r->f1_of_xx1__DD11[i1] = -sin(y);
   }
-  for (int i1 = 0; i1 < N1; i1++) {
-    const REAL y = xx[1][i1];
-    const REAL s = sin(y), c = cos(y);
+  for (int i1 = 0; i1 < N1; i1++)
     for (int i0 = 0; i0 < N0; i0++) {
-      const REAL x = xx[0][i0];
-      const REAL ep = exp(x / SINHWAA), em = exp(-x / SINHWAA);
-      const REAL A2 = pow(AMAX, 2) * pow(ep - em, 2) / pow(D, 2);
-      const REAL q = A2 + pow(bScale, 2) * pow(s, 2);
-      const REAL f2 = sqrt(q);
+      double o[5];
+      symtp_rfm_f2(AMAX, SINHWAA, bScale, xx[0][i0], xx[1][i1], o);
       const int k = i0 + N0 * i1;
-      r->f2_of_xx0_xx1[k] = f2;
-      r->f2_of_xx0_xx1__D0[k] =
-          (1.0 / 2.0) * pow(AMAX, 2) * (2 * ep / SINHWAA + 2 * em / SINHWAA) * (ep - em) / (f2 * pow(D, 2));
-      r->f2_of_xx0_xx1__D1[k] = pow(bScale, 2) * s * c / f2;
-      r->f2_of_xx0_xx1__DD00[k] =
-          -1.0 / 4.0 * pow(AMAX, 4) * pow(2 * ep / SINHWAA + 2 * em / SINHWAA, 2) * pow(ep - em, 2) /
-              (pow(q, 3.0 / 2.0) * pow(D, 4)) +
-          (1.0 / 2.0) * pow(AMAX, 2) * (2 * ep / pow(SINHWAA, 2) - 2 * em / pow(SINHWAA, 2)) * (ep - em) / (f2 * pow(D, 2)) +
-          (1.0 / 2.0) * pow(AMAX, 2) * (ep / SINHWAA + em / SINHWAA) * (2 * ep / SINHWAA + 2 * em / SINHWAA) / (f2 * pow(D, 2));
-      r->f2_of_xx0_xx1__DD11[k] = -pow(bScale, 4) * pow(s, 2) * pow(c, 2) / pow(q, 3.0 / 2.0) -
-                                   pow(bScale, 2) * pow(s, 2) / f2 + pow(bScale, 2) * pow(c, 2) / f2;
+      r->f2_of_xx0_xx1[k] = o[0];
+      r->f2_of_xx0_xx1__D0[k] = o[1];
+      r->f2_of_xx0_xx1__D1[k] = o[2];
+      r->f2_of_xx0_xx1__DD00[k] = o[3];
+      r->f2_of_xx0_xx1__DD11[k] = o[4];
     }
-  }
 }
 
 // find_timestep.c:5-46.  The reference returns the smallest proper grid

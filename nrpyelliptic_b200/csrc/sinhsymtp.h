@@ -140,4 +140,114 @@ NRPYELL_HD void symtp_ghost_source(int i0, int i1, int i2, int Nxx1, int Nxx2, i
   out[2] = j + NG;
 }
 
+// Reference-metric scale factors at one xx0 (rfm_precompute_rfmstruct_define.c:5-93).
+// With E(x) = exp(x/w) - exp(-x/w), D = exp(1/w) - exp(-1/w), A = AMAX E/D:
+// o = {f0 = A, d f0, d2 f0, d3 f0, f3 = sqrt(A^2 + b^2), d f3, d2 f3} (d = d/d xx0).
+NRPYELL_HD void symtp_rfm_xx0(double AMAX, double SINHWAA, double bScale, double x, double o[7]) {
+  const double D = exp(1.0 / SINHWAA) - exp(-1 / SINHWAA);
+  const double ep = exp(x / SINHWAA), em = exp(-x / SINHWAA);
+  o[0] = AMAX * (ep - em) / D;
+  o[1] = AMAX * (ep / SINHWAA + em / SINHWAA) / D;
+  o[2] = AMAX * (ep / pow(SINHWAA, 2) - em / pow(SINHWAA, 2)) / D;
+  o[3] = AMAX * (ep / pow(SINHWAA, 3) + em / pow(SINHWAA, 3)) / D;
+  const double A2 = pow(AMAX, 2) * pow(ep - em, 2) / pow(D, 2);
+  const double f3 = sqrt(A2 + pow(bScale, 2));
+  const double dA2 = (1.0 / 2.0) * pow(AMAX, 2) * (2 * ep / SINHWAA + 2 * em / SINHWAA) * (ep - em);  // (A^2)'/2 * D^2
+  o[4] = f3;
+  o[5] = dA2 / (f3 * pow(D, 2));
+  o[6] = -1.0 / 4.0 * pow(AMAX, 4) * pow(2 * ep / SINHWAA + 2 * em / SINHWAA, 2) * pow(ep - em, 2) /
+             (pow(A2 + pow(bScale, 2), 3.0 / 2.0) * pow(D, 4)) +
+         (1.0 / 2.0) * pow(AMAX, 2) * (2 * ep / pow(SINHWAA, 2) - 2 * em / pow(SINHWAA, 2)) * (ep - em) / (f3 * pow(D, 2)) +
+         (1.0 / 2.0) * pow(AMAX, 2) * (ep / SINHWAA + em / SINHWAA) * (2 * ep / SINHWAA + 2 * em / SINHWAA) / (f3 * pow(D, 2));
+}
+
+// f2 = sqrt(A^2 + b^2 sin^2 xx1) and its derivatives at (xx0, xx1):
+// o = {f2, d f2/d xx0, d f2/d xx1, d2 f2/d xx0^2, d2 f2/d xx1^2}.
+NRPYELL_HD void symtp_rfm_f2(double AMAX, double SINHWAA, double bScale, double x, double y, double o[5]) {
+  const double D = exp(1.0 / SINHWAA) - exp(-1 / SINHWAA);
+  const double s = sin(y), c = cos(y);
+  const double ep = exp(x / SINHWAA), em = exp(-x / SINHWAA);
+  const double A2 = pow(AMAX, 2) * pow(ep - em, 2) / pow(D, 2);
+  const double q = A2 + pow(bScale, 2) * pow(s, 2);
+  const double f2 = sqrt(q);
+  o[0] = f2;
+  o[1] = (1.0 / 2.0) * pow(AMAX, 2) * (2 * ep / SINHWAA + 2 * em / SINHWAA) * (ep - em) / (f2 * pow(D, 2));
+  o[2] = pow(bScale, 2) * s * c / f2;
+  o[3] = -1.0 / 4.0 * pow(AMAX, 4) * pow(2 * ep / SINHWAA + 2 * em / SINHWAA, 2) * pow(ep - em, 2) /
+             (pow(q, 3.0 / 2.0) * pow(D, 4)) +
+         (1.0 / 2.0) * pow(AMAX, 2) * (2 * ep / pow(SINHWAA, 2) - 2 * em / pow(SINHWAA, 2)) * (ep - em) / (f2 * pow(D, 2)) +
+         (1.0 / 2.0) * pow(AMAX, 2) * (ep / SINHWAA + em / SINHWAA) * (2 * ep / SINHWAA + 2 * em / SINHWAA) / (f2 * pow(D, 2));
+  o[4] = -pow(bScale, 4) * pow(s, 2) * pow(c, 2) / pow(q, 3.0 / 2.0) - pow(bScale, 2) * pow(s, 2) / f2 +
+         pow(bScale, 2) * pow(c, 2) / f2;
+}
+
+// The metric factors of the vv right-hand side (rhs_eval.c:106-110) folded
+// into one weight per raw stencil sum (ix = 1/dxx): cs = {d22 weight, d00
+// weight, d11 weight, d1 weight, d0 weight, centre weight}.
+NRPYELL_HD void symtp_fold_rhs_coefs(double f0, double f0p, double f0pp, double f1, double f1p, double f2,
+                                     double f2_0, double f3, double f3p, double ix0, double ix1, double ix2,
+                                     double cs[6]) {
+  const double P0 = 1.0 / (f2 * f2);
+  const double P2 = (f3 * f3) / (f0p * f0p);
+  const double P3 = 1.0 / ((f2 * f2) * f2);
+  const double ta = ((P0 * -1.0) * ((f3 * f3) / f0p)) / f0;
+  const double tb = P2 * (P3 * f2_0) - ta;
+  const double tc = (f3 * (f0p * f2_0 + f0pp * f2) - f0p * (f2 * f3p)) / ((f0p * f0p) * f0p);
+  const double td = (P3 * f3) * tc - tb;
+  const double c22 = ((1.0 / (f1 * f1)) / (f0 * f0)) * (ix2 * ix2);
+  const double c00 = P0 * P2 * (ix0 * ix0);
+  const double c11 = P0 * (ix1 * ix1);
+  cs[0] = c22;
+  cs[1] = c00;
+  cs[2] = c11;
+  cs[3] = (P0 * f1p / f1) * ix1;
+  cs[4] = -td * ix0;
+  cs[5] = -(5269.0 / 1800.0) * (c00 + c11 + c22);
+}
+
+// r and (d xx0/d r, d xx1/d r) at fixed spherical angles, for SinhSymTP at
+// (xx0, xx1); the azimuthal component is zero.  The reference evaluates a
+// generated closed form (apply_bcs_outerradiation_and_inner.c:290-321); the
+// same quantities follow from inverting the 2x2 Jacobian of
+// (r, zeta = z/r) with respect to (xx0, xx1):
+//   r^2 = A^2 + b^2 cos^2 xx1,  z = sqrt(A^2+b^2) cos xx1,
+//   d r/d xx0 = A A'/r,          d r/d xx1 = -b^2 sin xx1 cos xx1 / r,
+//   d zeta = (d z - zeta d r)/r,
+//   d xx0/d r = (d zeta/d xx1)/det,  d xx1/d r = -(d zeta/d xx0)/det.
+NRPYELL_HD void symtp_radial_geometry(double AMAX, double SINHWAA, double bScale, double xx0, double xx1,
+                                      double* r_out, double* dx0dr, double* dx1dr) {
+  const double iw = 1.0 / SINHWAA;
+  const double D = exp(iw) - exp(-iw);
+  const double ep = exp(iw * xx0), em = exp(-iw * xx0);
+  const double A = AMAX * (ep - em) / D;
+  const double Ap = AMAX * (iw * ep + iw * em) / D;
+  const double s = sin(xx1), c = cos(xx1);
+  const double b2 = bScale * bScale;
+  const double B = sqrt(A * A + b2);
+  const double r = sqrt(A * A * s * s + (A * A + b2) * c * c);
+  const double drdx0 = A * Ap / r;
+  const double drdx1 = -b2 * s * c / r;
+  const double z = B * c;
+  const double zeta = z / r;
+  const double dzdx0 = A * Ap * c / B;
+  const double dzdx1 = -B * s;
+  const double dzetadx0 = (dzdx0 - zeta * drdx0) / r;
+  const double dzetadx1 = (dzdx1 - zeta * drdx1) / r;
+  const double det = drdx0 * dzetadx1 - drdx1 * dzetadx0;
+  *r_out = r;
+  *dx0dr = dzetadx1 / det;
+  *dx1dr = -dzetadx0 / det;
+}
+
+// Upwind offset rule of compute_partial_r_f
+// (apply_bcs_outerradiation_and_inner.c:352-360), stencil radius 5.
+NRPYELL_HD int radiation_upwind_offset(int face, int i, int n) {
+  int off = face;
+  if (i < 5)
+    off = 5 - i;
+  else if (i > n - 5 - 1)
+    off = (n - 5 - 1) - i;
+  return off;
+}
+
 #endif

@@ -30,63 +30,20 @@ void upload(void* dst, const void* src, size_t bytes) {
   if (bytes) NRPYELL_CUDA(cudaMemcpy(dst, src, bytes, cudaMemcpyHostToDevice));
 }
 
-// r and (d xx0/d r, d xx1/d r) at fixed spherical angles, for SinhSymTP at
-// (xx0, xx1); the azimuthal component is zero.  The reference evaluates a
-// generated closed form (apply_bcs_outerradiation_and_inner.c:290-321); the
-// same quantities follow from inverting the 2x2 Jacobian of
-// (r, zeta = z/r) with respect to (xx0, xx1):
-//   r^2 = A^2 + b^2 cos^2 xx1,  z = sqrt(A^2+b^2) cos xx1,
-//   d r/d xx0 = A A'/r,          d r/d xx1 = -b^2 sin xx1 cos xx1 / r,
-//   d zeta = (d z - zeta d r)/r,
-//   d xx0/d r = (d zeta/d xx1)/det,  d xx1/d r = -(d zeta/d xx0)/det.
-void radial_geometry(double AMAX, double SINHWAA, double bScale, double xx0, double xx1, double* r_out,
-                     double* dx0dr, double* dx1dr) {
-  const double iw = 1.0 / SINHWAA;
-  const double D = exp(iw) - exp(-iw);
-  const double ep = exp(iw * xx0), em = exp(-iw * xx0);
-  const double A = AMAX * (ep - em) / D;
-  const double Ap = AMAX * (iw * ep + iw * em) / D;
-  const double s = sin(xx1), c = cos(xx1);
-  const double b2 = bScale * bScale;
-  const double B = sqrt(A * A + b2);
-  const double r = sqrt(A * A * s * s + (A * A + b2) * c * c);
-  const double drdx0 = A * Ap / r;
-  const double drdx1 = -b2 * s * c / r;
-  const double z = B * c;
-  const double zeta = z / r;
-  const double dzdx0 = A * Ap * c / B;
-  const double dzdx1 = -B * s;
-  const double dzetadx0 = (dzdx0 - zeta * drdx0) / r;
-  const double dzetadx1 = (dzdx1 - zeta * drdx1) / r;
-  const double det = drdx0 * dzetadx1 - drdx1 * dzetadx0;
-  *r_out = r;
-  *dx0dr = dzetadx1 / det;
-  *dx1dr = -dzetadx0 / det;
-}
-
-// Upwind offset rule of compute_partial_r_f
-// (apply_bcs_outerradiation_and_inner.c:352-360), stencil radius 5.
-int upwind_offset(int face, int i, int n) {
-  int off = face;
-  if (i < 5)
-    off = 5 - i;
-  else if (i > n - 5 - 1)
-    off = (n - 5 - 1) - i;
-  return off;
-}
 }  // namespace
 
-RfmTables* get_rfm_tables(const paramstruct* p, const rfm_struct* rfm) {
+RfmTables* find_rfm_tables(const paramstruct* p, const rfm_struct* rfm) {
   const Dims d = dims_of(p);
   for (RfmTables* t : g_rfm)
     if (t->key_f0 == rfm->f0_of_xx0 && t->key_f2 == rfm->f2_of_xx0_xx1 && same_dims(t->d, d) &&
         t->invdx[0] == p->invdx0 && t->invdx[1] == p->invdx1 && t->invdx[2] == p->invdx2 && t->AMAX == p->AMAX &&
         t->SINHWAA == p->SINHWAA && t->bScale == p->bScale)
       return t;
-  if (!rfm->f0_of_xx0 || !rfm->f2_of_xx0_xx1 || !rfm->f1_of_xx1 || !rfm->f3_of_xx0) {
-    NRPYELL_FAIL("rfm_struct has NULL arrays (call rfm_precompute_rfmstruct_define first)");
-    return nullptr;
-  }
+  return nullptr;
+}
+
+RfmTables* new_rfm_tables(const paramstruct* p, const rfm_struct* rfm) {
+  const Dims d = dims_of(p);
   RfmTables* t = new RfmTables();
   t->key_f0 = rfm->f0_of_xx0;
   t->key_f2 = rfm->f2_of_xx0_xx1;
@@ -98,9 +55,14 @@ RfmTables* get_rfm_tables(const paramstruct* p, const rfm_struct* rfm) {
   t->SINHWAA = p->SINHWAA;
   t->bScale = p->bScale;
   const size_t n0 = d.N0, n1 = d.N1, n01 = n0 * n1;
+  // the device build stages xx0 and xx1 behind the float weights
   const size_t n_doubles = 5 * n0 + 2 * n1 + 2 * n01 + kNumCoef * n01;
-  const size_t bytes = n_doubles * sizeof(double) + kNumCoef * n01 * sizeof(float) + 256;
+  const size_t bytes = n_doubles * sizeof(double) + kNumCoef * n01 * sizeof(float) + (n0 + n1) * sizeof(double) + 512;
   char* base = (char*)table_alloc(bytes);
+  if (!base) {
+    delete t;
+    return nullptr;
+  }
   t->base = base;
   double* q = (double*)base;
   t->f0 = q; q += n0;
@@ -114,6 +76,22 @@ RfmTables* get_rfm_tables(const paramstruct* p, const rfm_struct* rfm) {
   t->f2_D0 = q; q += n01;
   t->coef = q; q += kNumCoef * n01;
   t->coef32 = (float*)q;
+  t->xx01 = (double*)(base + ((n_doubles * sizeof(double) + kNumCoef * n01 * sizeof(float) + 255) / 256) * 256);
+  return t;
+}
+
+void register_rfm_tables(RfmTables* t) { g_rfm.push_back(t); }
+
+RfmTables* get_rfm_tables(const paramstruct* p, const rfm_struct* rfm) {
+  if (RfmTables* f = find_rfm_tables(p, rfm)) return f;
+  if (!rfm->f0_of_xx0 || !rfm->f2_of_xx0_xx1 || !rfm->f1_of_xx1 || !rfm->f3_of_xx0) {
+    NRPYELL_FAIL("rfm_struct has NULL arrays (call rfm_precompute_rfmstruct_define or nrpyell_setup_tables_device first)");
+    return nullptr;
+  }
+  RfmTables* t = new_rfm_tables(p, rfm);
+  if (!t) return nullptr;
+  const Dims d = t->d;
+  const size_t n0 = d.N0, n1 = d.N1, n01 = n0 * n1;
   upload(t->f0, rfm->f0_of_xx0, n0 * 8);
   upload(t->f0_D0, rfm->f0_of_xx0__D0, n0 * 8);
   upload(t->f0_DD00, rfm->f0_of_xx0__DD00, n0 * 8);
@@ -136,20 +114,8 @@ RfmTables* get_rfm_tables(const paramstruct* p, const rfm_struct* rfm) {
       const double f1 = rfm->f1_of_xx1[i1], f1p = rfm->f1_of_xx1__D1[i1];
       const double f2 = rfm->f2_of_xx0_xx1[k], f2_0 = rfm->f2_of_xx0_xx1__D0[k];
       const double f3 = rfm->f3_of_xx0[i0], f3p = rfm->f3_of_xx0__D0[i0];
-      const double P0 = 1.0 / (f2 * f2);
-      const double P2 = (f3 * f3) / (f0p * f0p);
-      const double P3 = 1.0 / ((f2 * f2) * f2);
-      const double ta = ((P0 * -1.0) * ((f3 * f3) / f0p)) / f0;
-      const double tb = P2 * (P3 * f2_0) - ta;
-      const double tc = (f3 * (f0p * f2_0 + f0pp * f2) - f0p * (f2 * f3p)) / ((f0p * f0p) * f0p);
-      const double td = (P3 * f3) * tc - tb;
-      const double c22 = ((1.0 / (f1 * f1)) / (f0 * f0)) * (ix2 * ix2);
-      const double c00 = P0 * P2 * (ix0 * ix0);
-      const double c11 = P0 * (ix1 * ix1);
-      const double c1 = (P0 * f1p / f1) * ix1;
-      const double c0 = -td * ix0;
-      const double cc = -(5269.0 / 1800.0) * (c00 + c11 + c22);
-      const double cs[kNumCoef] = {c22, c00, c11, c1, c0, cc};
+      double cs[kNumCoef];
+      symtp_fold_rhs_coefs(f0, f0p, f0pp, f1, f1p, f2, f2_0, f3, f3p, ix0, ix1, ix2, cs);
       for (int c = 0; c < kNumCoef; c++) {
         coef[c * n01 + k] = cs[c];
         coef32[c * n01 + k] = (float)cs[c];
@@ -161,7 +127,7 @@ RfmTables* get_rfm_tables(const paramstruct* p, const rfm_struct* rfm) {
   return t;
 }
 
-BcTables* get_bc_tables(const paramstruct* p, const bc_struct* bc, REAL* NRPYELL_RESTRICT const xx[3]) {
+BcTables* find_bc_tables(const paramstruct* p, const bc_struct* bc, REAL* NRPYELL_RESTRICT const xx[3]) {
   const Dims d = dims_of(p);
   for (BcTables* t : g_bc)
     if (t->key_inner == bc->inner_bc_array && t->key_outer0 == bc->pure_outer_bc_array[0] &&
@@ -169,6 +135,46 @@ BcTables* get_bc_tables(const paramstruct* p, const bc_struct* bc, REAL* NRPYELL
         t->key_xx[1] == xx[1] && t->key_xx[2] == xx[2] && t->AMAX == p->AMAX && t->SINHWAA == p->SINHWAA &&
         t->bScale == p->bScale && t->dxx0 == p->dxx0 && t->dxx1 == p->dxx1 && t->dxx2 == p->dxx2)
       return t;
+  return nullptr;
+}
+
+void register_bc_tables(BcTables* t) { g_bc.push_back(t); }
+
+void bc_tables_set_key(BcTables* t, const paramstruct* p, const bc_struct* bc, REAL* NRPYELL_RESTRICT const xx[3]) {
+  t->key_inner = bc->inner_bc_array;
+  t->key_outer0 = bc->pure_outer_bc_array[0];
+  t->key_ninner = bc->bc_info.num_inner_boundary_points;
+  for (int i = 0; i < 3; i++) t->key_xx[i] = xx[i];
+  t->d = dims_of(p);
+  t->AMAX = p->AMAX;
+  t->SINHWAA = p->SINHWAA;
+  t->bScale = p->bScale;
+  t->dxx0 = p->dxx0;
+  t->dxx1 = p->dxx1;
+  t->dxx2 = p->dxx2;
+}
+
+bool bc_tables_layout(BcTables* t, size_t n_inner, size_t n_outer) {
+  const size_t b_inner = (n_inner > 0 ? n_inner : 1) * sizeof(int2);
+  const size_t b_par = (((n_inner > 0 ? n_inner : 1) + 255) / 256) * 256;
+  const size_t b_outer = (n_outer > 0 ? n_outer : 1) * sizeof(OuterPoint);
+  const size_t b_col = 3 * 6 * (size_t)t->d.N1 * sizeof(double);
+  const size_t b_xx = ((size_t)t->d.N0 + t->d.N1) * sizeof(double);
+  char* base = (char*)table_alloc(b_inner + b_par + b_outer + b_col + b_xx + 1280);
+  if (!base) return false;
+  t->base = base;
+  size_t o = 0;
+  t->inner = (int2*)(base + o); o += (b_inner + 255) / 256 * 256;
+  t->inner_par = (signed char*)(base + o); o += b_par;
+  t->outer = (OuterPoint*)(base + o); o += (b_outer + 255) / 256 * 256;
+  t->colgeo = (double*)(base + o); o += (b_col + 255) / 256 * 256;
+  t->xx01 = (double*)(base + o);
+  return true;
+}
+
+BcTables* get_bc_tables(const paramstruct* p, const bc_struct* bc, REAL* NRPYELL_RESTRICT const xx[3]) {
+  if (BcTables* f = find_bc_tables(p, bc, xx)) return f;
+  const Dims d = dims_of(p);
   BcTables* t = new BcTables();
   t->key_inner = bc->inner_bc_array;
   t->key_outer0 = bc->pure_outer_bc_array[0];
@@ -243,13 +249,13 @@ BcTables* get_bc_tables(const paramstruct* p, const bc_struct* bc, REAL* NRPYELL
           columns_ok = false;
         q.idx3 = o.i0 + N0 * (o.i1 + N1 * o.i2);
         q.idx3_int = q.i0n + N0 * (q.i1n + N1 * q.i2n);
-        q.off0 = (signed char)upwind_offset(o.FACEX0, o.i0, N0);
-        q.off1 = (signed char)upwind_offset(o.FACEX1, o.i1, N1);
-        q.off0n = (signed char)upwind_offset(o.FACEX0, q.i0n, N0);
-        q.off1n = (signed char)upwind_offset(o.FACEX1, q.i1n, N1);
+        q.off0 = (signed char)radiation_upwind_offset(o.FACEX0, o.i0, N0);
+        q.off1 = (signed char)radiation_upwind_offset(o.FACEX1, o.i1, N1);
+        q.off0n = (signed char)radiation_upwind_offset(o.FACEX0, q.i0n, N0);
+        q.off1n = (signed char)radiation_upwind_offset(o.FACEX1, q.i1n, N1);
         if (xx[0] && xx[1]) {
-          radial_geometry(p->AMAX, p->SINHWAA, p->bScale, xx[0][o.i0], xx[1][o.i1], &q.r, &q.dx0dr, &q.dx1dr);
-          radial_geometry(p->AMAX, p->SINHWAA, p->bScale, xx[0][q.i0n], xx[1][q.i1n], &q.rn, &q.dx0drn, &q.dx1drn);
+          symtp_radial_geometry(p->AMAX, p->SINHWAA, p->bScale, xx[0][o.i0], xx[1][o.i1], &q.r, &q.dx0dr, &q.dx1dr);
+          symtp_radial_geometry(p->AMAX, p->SINHWAA, p->bScale, xx[0][q.i0n], xx[1][q.i1n], &q.rn, &q.dx0drn, &q.dx1drn);
         } else {
           q.r = q.dx0dr = q.dx1dr = q.rn = q.dx0drn = q.dx1drn = 0.0;
         }
@@ -268,27 +274,20 @@ BcTables* get_bc_tables(const paramstruct* p, const bc_struct* bc, REAL* NRPYELL
   for (int j = 0; j < 6 && t->columns_ok; j++)
     for (int i1 = 0; i1 < N1; i1++) {
       double r, a, b;
-      radial_geometry(p->AMAX, p->SINHWAA, p->bScale, xx[0][N0 - NGHOSTS - 1 + j], xx[1][i1], &r, &a, &b);
+      symtp_radial_geometry(p->AMAX, p->SINHWAA, p->bScale, xx[0][N0 - NGHOSTS - 1 + j], xx[1][i1], &r, &a, &b);
       colgeo[(0 * 6 + j) * N1 + i1] = r;
       colgeo[(1 * 6 + j) * N1 + i1] = a;
       colgeo[(2 * 6 + j) * N1 + i1] = b;
     }
 
-  const size_t b_inner = inner.size() * sizeof(int2);
-  const size_t b_par = ((par.size() + 255) / 256) * 256;
-  const size_t b_outer = (outer.size() > 0 ? outer.size() : 1) * sizeof(OuterPoint);
-  const size_t b_col = colgeo.size() * sizeof(double);
-  char* base = (char*)table_alloc(b_inner + b_par + b_outer + b_col + 1024);
-  t->base = base;
-  size_t o = 0;
-  t->inner = (int2*)(base + o); o += (b_inner + 255) / 256 * 256;
-  t->inner_par = (signed char*)(base + o); o += b_par;
-  t->outer = (OuterPoint*)(base + o); o += (b_outer + 255) / 256 * 256;
-  t->colgeo = (double*)(base + o);
-  upload(t->inner, inner.data(), b_inner);
+  if (!bc_tables_layout(t, inner.size(), outer.size())) {
+    delete t;
+    return nullptr;
+  }
+  upload(t->inner, inner.data(), inner.size() * sizeof(int2));
   upload(t->inner_par, par.data(), par.size());
   if (!outer.empty()) upload(t->outer, outer.data(), outer.size() * sizeof(OuterPoint));
-  upload(t->colgeo, colgeo.data(), b_col);
+  upload(t->colgeo, colgeo.data(), colgeo.size() * sizeof(double));
   g_bc.push_back(t);
   return t;
 }

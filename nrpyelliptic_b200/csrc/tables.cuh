@@ -41,6 +41,7 @@ struct RfmTables {
   //   5: centre weight  -(5269/1800) (c0 + c1 + c2)
   double* coef;
   float* coef32;
+  double* xx01;  // device build: xx0 [N0] then xx1 [N1]
   void* base;
 };
 
@@ -82,6 +83,7 @@ struct BcTables {
   // geometry for the column form, [6][N1]: j=0 is the last interior plane,
   // j=1..5 the outer layers; arrays r, dx0dr, dx1dr
   double* colgeo;
+  double* xx01;  // xx0 [N0] then xx1 [N1] on the device (bc_tables_layout)
   void* base;
 };
 
@@ -94,6 +96,16 @@ struct L2Tables {
 };
 
 RfmTables* get_rfm_tables(const paramstruct* p, const rfm_struct* rfm);
+// Cache lookup only (nullptr when absent), allocation and layout of a new
+// entry keyed by rfm / bc, and registration of a filled entry -- shared by
+// the host build (get_*_tables) and the device build (tables_gpu.cu).
+RfmTables* find_rfm_tables(const paramstruct* p, const rfm_struct* rfm);
+RfmTables* new_rfm_tables(const paramstruct* p, const rfm_struct* rfm);
+void register_rfm_tables(RfmTables* t);
+BcTables* find_bc_tables(const paramstruct* p, const bc_struct* bc, REAL* NRPYELL_RESTRICT const xx[3]);
+void bc_tables_set_key(BcTables* t, const paramstruct* p, const bc_struct* bc, REAL* NRPYELL_RESTRICT const xx[3]);
+bool bc_tables_layout(BcTables* t, size_t n_inner, size_t n_outer);
+void register_bc_tables(BcTables* t);
 BcTables* get_bc_tables(const paramstruct* p, const bc_struct* bc, REAL* NRPYELL_RESTRICT const xx[3]);
 L2Tables* get_l2_tables(const paramstruct* p, REAL* NRPYELL_RESTRICT const xx[3], double R);
 void release_all_tables();

@@ -51,7 +51,7 @@ def solve_snapshots(cfgs, lib, chunk=64, tol=-10.0, max_steps=40000, log=print):
     converged uu arrays (float32, ghost zones included) and step counts."""
     snaps, steps = None, []
     for c0 in range(0, len(cfgs), chunk):
-        probs = [Problem(c, lib=lib, host_aux=False) for c in cfgs[c0:c0 + chunk]]
+        probs = [Problem(c, lib=lib, host_aux=False, device_tables=True) for c in cfgs[c0:c0 + chunk]]
         rc, st, _, states = relax_batch(probs, tol=tol, max_steps=max_steps, lib=lib)
         if snaps is None:
             snaps = np.empty((len(cfgs), probs[0].Ntot), np.float32)
@@ -197,7 +197,7 @@ def evaluate(lib, guess, cfgs, log=print):
     rows, zeros = [], []
     coeffs = guess.predict([features(c) for c in cfgs])
     for i, cfg in enumerate(cfgs):
-        prob = Problem(cfg, lib=lib, host_aux=False)
+        prob = Problem(cfg, lib=lib, host_aux=False, device_tables=True)
         ds = DeviceState(prob, lib=lib)
         r0 = initial_log10_l2(lib, prob, ds)
         s0, t0, f0 = timed_relax(lib, prob, ds, False)
@@ -240,7 +240,7 @@ def compare_solvers(lib, guess, cfgs, log=print):
     fallback test are inside (b)-(d).  Returns a dict of solves/s, RK4 steps
     and the speed-up of each form over (a)."""
     from .batch import relax_batch
-    probs = [Problem(c, lib=lib, host_aux=False) for c in cfgs]
+    probs = [Problem(c, lib=lib, host_aux=False, device_tables=True) for c in cfgs]
     states = [DeviceState(p, lib=lib) for p in probs]
     n = len(cfgs)
     out = {"configurations": n}

@@ -118,8 +118,9 @@ class Problem:
     auxevol gridfunctions and dt.  Arrays are numpy views of C memory owned
     by this object (freed in close())."""
 
-    def __init__(self, cfg, lib=None, host_aux=True):
+    def __init__(self, cfg, lib=None, host_aux=True, device_tables=False):
         self.cfg = cfg
+        self.device_tables = device_tables
         self.lib = lib = lib or _lib.load()
         p = abi.paramstruct()
         lib.nrpyell_set_Cparameters_to_default(C.byref(p))
@@ -129,11 +130,14 @@ class Problem:
         lib.nrpyell_set_Nxx_dxx_invdx_params__and__xx(0, nxx, C.byref(p), self.xx)
         self.params = p
         self.bc = abi.bc_struct()
-        lib.nrpyell_bcstruct_set_up(C.byref(p), C.byref(self.bc))
-        self.dt = lib.nrpyell_find_timestep(C.byref(p), self.xx, cfg.CFL)
         self.rfm = abi.rfm_struct()
-        lib.nrpyell_rfm_precompute_rfmstruct_malloc(C.byref(p), C.byref(self.rfm))
-        lib.nrpyell_rfm_precompute_rfmstruct_define(C.byref(p), self.xx, C.byref(self.rfm))
+        self.dt = lib.nrpyell_find_timestep(C.byref(p), self.xx, cfg.CFL)
+        if not device_tables:
+            lib.nrpyell_bcstruct_set_up(C.byref(p), C.byref(self.bc))
+            lib.nrpyell_rfm_precompute_rfmstruct_malloc(C.byref(p), C.byref(self.rfm))
+            lib.nrpyell_rfm_precompute_rfmstruct_define(C.byref(p), self.xx, C.byref(self.rfm))
+        # else: bc and rfm stay empty; DeviceState builds the device tables
+        # on the GPU (nrpyell_setup_tables_device) keyed by these structs
         self.N = (p.Nxx_plus_2NGHOSTS0, p.Nxx_plus_2NGHOSTS1, p.Nxx_plus_2NGHOSTS2)
         self.Ntot = self.N[0] * self.N[1] * self.N[2]
         self._closed = False
@@ -243,6 +247,11 @@ class DeviceState:
         for k in ("acc", "k_odd", "k_even"):
             lib.nrpyell_memset(self.ptr[k], 0, n2)
         self.g = prob.griddata(self.ptr)
+        if prob.device_tables:
+            # the griddata struct holds copies of bc / rfm: key the tables by those
+            lib.nrpyell_setup_tables_device(C.byref(prob.params), prob.xx, C.byref(self.g.rfmstruct),
+                                            C.byref(self.g.bcstruct))
+            _lib.check(lib)
 
     def upload(self, key, arr):
         arr = np.ascontiguousarray(arr, dtype=np.float64)
