@@ -46,9 +46,25 @@ def configs(n, seed):
     return [with_grid(c, GRID) for c in sample_sweep(n, seed)]
 
 
-def solve_snapshots(cfgs, lib, chunk=64, tol=-10.0, max_steps=40000, log=print):
+def solve_snapshots(cfgs, lib, chunk=64, tol=-10.0, max_steps=40000, log=print, dist=None):
     """Relax every configuration from the zero guess in batches; returns the
-    converged uu arrays (float32, ghost zones included) and step counts."""
+    converged uu arrays (float32, ghost zones included) and step counts.
+    With `dist` (replicas.Replicas, one process per GPU) the configurations
+    are dealt round-robin over the ranks, each rank solves its share, and the
+    snapshots are gathered on the host of every rank."""
+    if dist is not None and dist.world > 1:
+        from .replicas import shard
+        mine = shard(list(range(len(cfgs))), dist.rank, dist.world)
+        part = solve_snapshots([cfgs[i] for i in mine], lib, chunk, tol, max_steps, log) if mine else (None, [])
+        parts = dist.all_gather((mine, part[0], list(part[1])))
+        ntot = next(p[1].shape[1] for p in parts if p[1] is not None)
+        snaps = np.empty((len(cfgs), ntot), np.float32)
+        steps = np.zeros(len(cfgs), np.int64)
+        for idx, sn, st in parts:
+            for k, i in enumerate(idx):
+                snaps[i] = sn[k]
+                steps[i] = st[k]
+        return snaps, steps
     snaps, steps = None, []
     for c0 in range(0, len(cfgs), chunk):
         probs = [Problem(c, lib=lib, host_aux=False, device_tables=True) for c in cfgs[c0:c0 + chunk]]

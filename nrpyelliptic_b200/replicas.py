@@ -4,8 +4,9 @@ A single relaxation does not shard across GPUs (the inner boundary gathers
 across the axis and the RK4 stages are sequential), so multi-GPU runs solve
 independent puncture configurations per rank: no collective touches the data
 path.  torch.distributed supplies only the plumbing around it -- a barrier
-before and after a timed region and the max of the per-rank times -- over
-NCCL on GPUs (gloo on CPU-only hosts and in the tests).
+before and after a timed region, the max of the per-rank times and the
+gathering of per-configuration results on the host after a sharded sweep --
+over NCCL on GPUs (gloo on CPU-only hosts and in the tests).
 """
 import datetime
 import os
@@ -51,6 +52,15 @@ class Replicas:
         t = self.torch.tensor([float(x)], dtype=self.torch.float64, device=self._device())
         self.dist.all_reduce(t, op=self.dist.ReduceOp.SUM)
         return float(t.item())
+
+    def all_gather(self, obj):
+        """Every rank's `obj` (picklable host data), in rank order, on every
+        rank -- for gathering per-configuration results after the solves."""
+        if not self.dist:
+            return [obj]
+        out = [None] * self.world
+        self.dist.all_gather_object(out, obj)
+        return out
 
     def close(self):
         if self.dist:
