@@ -1,14 +1,16 @@
 // Learned initial guess: a small MLP (puncture parameters -> POD coefficients
-// of uu) trained and evaluated on the GPU with BF16 tensor-core matrix
-// products (mma.sync m16n8k16, FP32 accumulation), FP32 master weights and
-// Adam; plus the POD reconstruction of the guess.
+// of uu) trained and evaluated on the GPU with BF16 matrix products on the
+// fifth-generation tensor cores (tcgen05.mma, FP32 accumulators in tensor
+// memory), FP32 master weights and Adam; plus the POD reconstruction of the
+// guess.
 //
 // Every matrix product of the network -- forward Z = H W, backward
-// dH = dZ W^T and dW = H^T dZ -- is one kernel, k_gemm_bf16: 64x64 output
-// tiles, four warps of 32x32, operands read with arbitrary strides (so the
-// transposes are free), rounded to BF16 into shared memory and multiplied
-// with FP32 accumulators, with the bias and tanh of the forward pass fused
-// into the epilogue.
+// dH = dZ W^T and dW = H^T dZ -- is one kernel, k_gemm_tc: 128 x 64 output
+// tiles, operands read with arbitrary strides (so the transposes are free),
+// rounded to BF16 into shared memory in the tensor cores' layout and
+// multiplied by tcgen05.mma issued from one thread, with the bias and tanh
+// of the forward pass fused into the epilogue that reads the accumulator
+// back with tcgen05.ld.
 #include <cuda_bf16.h>
 #include <math.h>
 #include <stdint.h>
@@ -25,102 +27,220 @@ namespace {
 // ------------------------------------------------------------------ GEMM
 // C[M x N] = alpha * A[M x K] B[K x N] (+ bias[N]) (then tanh), with
 // A(m,k) = A[m*sam + k*sak] and B(k,n) = B[k*sbk + n*sbn]; FP32 in and out.
-constexpr int GT = 64;  // output tile
-constexpr int GK = 16;  // k step (one mma)
+//
+// One CTA of 128 threads computes a 128 x 64 tile of C on the fifth-
+// generation tensor cores: the operands are rounded to BF16 and written to
+// shared memory in the tensor cores' no-swizzle K-major layout (8 x 8
+// core matrices of 128 contiguous bytes), one thread issues
+// tcgen05.mma.cta_group::1.kind::f16 (M = 128, N = 64, K = 16) with the
+// FP32 accumulator in tensor memory, tcgen05.commit signals an mbarrier when
+// the products of a 64-deep K chunk are done (the next chunk may then
+// overwrite shared memory), and each warp reads its 32 rows of the
+// accumulator back with tcgen05.ld for the epilogue (alpha, bias, tanh).
+constexpr int TC_M = 128, TC_N = 64, TC_KC = 64;      // CTA tile and K chunk
+constexpr int TC_B_OFF = 32 * 1024;                   // B tile at 32 KB (the 16 KB A tile at 0)
+constexpr int TC_SMEM = 64 * 1024;                    // dynamic shared memory per CTA
+constexpr int TC_TMEM_COLS = 128;                     // tensor-memory columns allocated (N = 64 used)
 constexpr int EPI_NONE = 0, EPI_BIAS = 1, EPI_BIAS_TANH = 2;
+constexpr long long kTcWaitLimit = 1ll << 22;         // bounded mbarrier wait (iterations)
 
 __device__ __forceinline__ uint32_t pack_bf16(float lo, float hi) {
   const __nv_bfloat16 l = __float2bfloat16_rn(lo), h = __float2bfloat16_rn(hi);
   return (uint32_t)__bfloat16_as_ushort(l) | ((uint32_t)__bfloat16_as_ushort(h) << 16);
 }
 
-__global__ void __launch_bounds__(128) k_gemm_bf16(int M, int N, int K, const float* __restrict__ A, long long sam,
-                                                  long long sak, const float* __restrict__ B, long long sbk,
-                                                  long long sbn, float* __restrict__ Cm, long long ldc,
-                                                  const float* __restrict__ bias, int epi, float alpha) {
-  // As[m][k/2], Bs[n][k/2]: BF16 pairs along k packed in 32 bits
-  __shared__ uint32_t As[GT][GK / 2 + 1];
-  __shared__ uint32_t Bs[GT][GK / 2 + 1];
-  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
-  const int m0 = blockIdx.y * GT, n0 = blockIdx.x * GT;
-  const int wm = (warp >> 1) * 32, wn = (warp & 1) * 32;  // warp tile origin
-  const int g = lane >> 2, t = lane & 3;
-  float acc[2][4][4];
-#pragma unroll
-  for (int i = 0; i < 2; i++)
-#pragma unroll
-    for (int j = 0; j < 4; j++)
-#pragma unroll
-      for (int r = 0; r < 4; r++) acc[i][j][r] = 0.f;
-  for (int k0 = 0; k0 < K; k0 += GK) {
-    // 64 x 8 packed pairs per operand, 128 threads: 4 pairs each
-    for (int e = tid; e < GT * GK / 2; e += 128) {
-      const int r = e / (GK / 2), kp = e % (GK / 2);
-      const int k = k0 + 2 * kp;
-      const int m = m0 + r, n = n0 + r;
-      float a0 = 0.f, a1 = 0.f, b0 = 0.f, b1 = 0.f;
-      if (m < M) {
-        if (k < K) a0 = A[m * sam + k * sak];
-        if (k + 1 < K) a1 = A[m * sam + (k + 1) * sak];
-      }
-      if (n < N) {
-        if (k < K) b0 = B[k * sbk + n * sbn];
-        if (k + 1 < K) b1 = B[(k + 1) * sbk + n * sbn];
-      }
-      As[r][kp] = pack_bf16(a0, a1);
-      Bs[r][kp] = pack_bf16(b0, b1);
-    }
-    __syncthreads();
-    // fragments of mma.m16n8k16 (row A, col B): lane (g, t) holds A rows g
-    // and g+8 at k = 2t, 2t+1 and 2t+8, 2t+9, B column g at the same k
-    uint32_t af[2][4], bfr[4][2];
-#pragma unroll
-    for (int i = 0; i < 2; i++) {
-      const int r = wm + 16 * i + g;
-      af[i][0] = As[r][t];
-      af[i][1] = As[r + 8][t];
-      af[i][2] = As[r][t + 4];
-      af[i][3] = As[r + 8][t + 4];
-    }
-#pragma unroll
-    for (int j = 0; j < 4; j++) {
-      const int c = wn + 8 * j + g;
-      bfr[j][0] = Bs[c][t];
-      bfr[j][1] = Bs[c][t + 4];
-    }
-#pragma unroll
-    for (int i = 0; i < 2; i++)
-#pragma unroll
-      for (int j = 0; j < 4; j++)
-        asm volatile(
-            "mma.sync.aligned.m16n8k16.row.col.f32.bf16.bf16.f32 {%0,%1,%2,%3}, {%4,%5,%6,%7}, {%8,%9}, "
-            "{%0,%1,%2,%3};\n"
-            : "+f"(acc[i][j][0]), "+f"(acc[i][j][1]), "+f"(acc[i][j][2]), "+f"(acc[i][j][3])
-            : "r"(af[i][0]), "r"(af[i][1]), "r"(af[i][2]), "r"(af[i][3]), "r"(bfr[j][0]), "r"(bfr[j][1]));
-    __syncthreads();
+__device__ __forceinline__ uint32_t smem_addr(const void* p) { return (uint32_t)__cvta_generic_to_shared(p); }
+
+// Shared-memory matrix descriptor of a no-swizzle K-major operand: start
+// address, leading-dimension byte offset (between core matrices adjacent in
+// K), stride-dimension byte offset (between core matrices adjacent in M/N),
+// descriptor version 1, layout type 0 (no swizzle).
+__device__ __forceinline__ uint64_t smem_desc(uint32_t addr, uint32_t lbo, uint32_t sbo) {
+  return (uint64_t)((addr >> 4) & 0x3FFF) | ((uint64_t)((lbo >> 4) & 0x3FFF) << 16) |
+         ((uint64_t)((sbo >> 4) & 0x3FFF) << 32) | (1ull << 46);
+}
+
+// Instruction descriptor of kind::f16: FP32 accumulator (bits 4-5 = 1), BF16 A
+// and B (bits 7-9, 10-12 = 1), both K-major (bits 15, 16 = 0), N >> 3 at bit
+// 17, M >> 4 at bit 24.
+constexpr uint32_t kTcIdesc = (1u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(TC_N >> 3) << 17) |
+                              ((uint32_t)(TC_M >> 4) << 24);
+
+// Byte offset of element (r, k) (r: M or N row, k: K index, even) of a tile
+// with R rows: core matrix (r/8, k/8) at ((k/8) * (R/8) + r/8) * 128, row r%8
+// at 16 bytes, element k%8 at 2 bytes.
+template <int R>
+__device__ __forceinline__ uint32_t tile_off(int r, int k) {
+  return (uint32_t)((((k >> 3) * (R / 8) + (r >> 3)) << 7) + ((r & 7) << 4) + ((k & 7) << 1));
+}
+
+__device__ __forceinline__ bool mbar_wait(uint32_t mbar, uint32_t parity) {
+  for (long long it = 0; it < kTcWaitLimit; it++) {
+    uint32_t done;
+    asm volatile(
+        "{\n.reg .pred p;\nmbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\nselp.u32 %0, 1, 0, p;\n}\n"
+        : "=r"(done)
+        : "r"(mbar), "r"(parity)
+        : "memory");
+    if (done) return true;
   }
-  // accumulator lane (g, t): rows g, g+8, columns 2t, 2t+1
+  return false;
+}
+
+__global__ void __launch_bounds__(128) k_gemm_tc(int M, int N, int K, const float* __restrict__ A, long long sam,
+                                                long long sak, const float* __restrict__ B, long long sbk,
+                                                long long sbn, float* __restrict__ Cm, long long ldc,
+                                                const float* __restrict__ bias, int epi, float alpha, int* err) {
+  extern __shared__ __align__(1024) unsigned char tc_smem[];
+  __shared__ __align__(8) unsigned long long mbar;
+  __shared__ uint32_t tmem_base;
+  __shared__ int failed;
+  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+  const int m0 = blockIdx.y * TC_M, n0 = blockIdx.x * TC_N;
+  unsigned char* As = tc_smem;
+  unsigned char* Bs = tc_smem + TC_B_OFF;
+  const uint32_t mb = smem_addr(&mbar);
+  if (warp == 0) {
+    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;\n" ::"r"(smem_addr(&tmem_base)),
+                 "n"(TC_TMEM_COLS)
+                 : "memory");
+    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;\n" ::: "memory");
+  }
+  if (tid == 0) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;\n" ::"r"(mb) : "memory");
+    failed = 0;
+  }
+  asm volatile("tcgen05.fence::before_thread_sync;\n" ::: "memory");
+  __syncthreads();
+  asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory");
+  const uint32_t tmem = tmem_base;
+  const int nchunks = (K + TC_KC - 1) / TC_KC;
+  for (int c = 0; c < nchunks; c++) {
+    const int k0 = c * TC_KC;
+    // A chunk: 128 rows x 32 k-pairs; B chunk: 64 rows (n) x 32 k-pairs
+    for (int e = tid; e < TC_M * TC_KC / 2; e += 128) {
+      const int r = e / (TC_KC / 2), k = 2 * (e % (TC_KC / 2));
+      const int m = m0 + r, kk = k0 + k;
+      float a0 = 0.f, a1 = 0.f;
+      if (m < M) {
+        if (kk < K) a0 = A[m * sam + kk * sak];
+        if (kk + 1 < K) a1 = A[m * sam + (kk + 1) * sak];
+      }
+      *reinterpret_cast<uint32_t*>(As + tile_off<TC_M>(r, k)) = pack_bf16(a0, a1);
+    }
+    for (int e = tid; e < TC_N * TC_KC / 2; e += 128) {
+      const int r = e / (TC_KC / 2), k = 2 * (e % (TC_KC / 2));
+      const int n = n0 + r, kk = k0 + k;
+      float b0 = 0.f, b1 = 0.f;
+      if (n < N) {
+        if (kk < K) b0 = B[kk * sbk + n * sbn];
+        if (kk + 1 < K) b1 = B[(kk + 1) * sbk + n * sbn];
+      }
+      *reinterpret_cast<uint32_t*>(Bs + tile_off<TC_N>(r, k)) = pack_bf16(b0, b1);
+    }
+    // make the generic-proxy writes visible to the tensor cores
+    asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory");
+    __syncthreads();
+    if (tid == 0) {
+      asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory");
 #pragma unroll
-  for (int i = 0; i < 2; i++)
+      for (int s = 0; s < TC_KC / 16; s++) {
+        // K sub-block s: core-matrix columns 2s and 2s+1
+        const uint64_t ad = smem_desc(smem_addr(As) + s * 2 * (TC_M / 8) * 128, (TC_M / 8) * 128, 128);
+        const uint64_t bd = smem_desc(smem_addr(Bs) + s * 2 * (TC_N / 8) * 128, (TC_N / 8) * 128, 128);
+        const uint32_t acc = (c > 0 || s > 0) ? 1u : 0u;
+        asm volatile(
+            "{\n.reg .pred p;\nsetp.ne.b32 p, %4, 0;\n"
+            "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n}\n" ::"r"(tmem),
+            "l"(ad), "l"(bd), "r"(kTcIdesc), "r"(acc)
+            : "memory");
+      }
+      asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];\n" ::"r"(mb)
+                   : "memory");
+    }
+    // the chunk's products are done before shared memory is rewritten
+    if (!mbar_wait(mb, (uint32_t)(c & 1))) failed = 1;
+    __syncthreads();
+    if (failed) break;
+  }
+  asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory");
+  if (!failed) {
+    // warp w reads accumulator rows 32w..32w+31 (tensor-memory lanes), 64 columns
+    const int m = m0 + 32 * warp + lane;
+    const uint32_t taddr = tmem + ((uint32_t)(32 * warp) << 16);
 #pragma unroll
-    for (int j = 0; j < 4; j++)
+    for (int half = 0; half < 2; half++) {
+      uint32_t v[32];
+      asm volatile(
+          "tcgen05.ld.sync.aligned.32x32b.x32.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15,%16,%17,%18,"
+          "%19,%20,%21,%22,%23,%24,%25,%26,%27,%28,%29,%30,%31}, [%32];\n"
+          : "=r"(v[0]), "=r"(v[1]), "=r"(v[2]), "=r"(v[3]), "=r"(v[4]), "=r"(v[5]), "=r"(v[6]), "=r"(v[7]),
+            "=r"(v[8]), "=r"(v[9]), "=r"(v[10]), "=r"(v[11]), "=r"(v[12]), "=r"(v[13]), "=r"(v[14]), "=r"(v[15]),
+            "=r"(v[16]), "=r"(v[17]), "=r"(v[18]), "=r"(v[19]), "=r"(v[20]), "=r"(v[21]), "=r"(v[22]), "=r"(v[23]),
+            "=r"(v[24]), "=r"(v[25]), "=r"(v[26]), "=r"(v[27]), "=r"(v[28]), "=r"(v[29]), "=r"(v[30]), "=r"(v[31])
+          : "r"(taddr + 32 * half));
+      asm volatile("tcgen05.wait::ld.sync.aligned;\n" ::: "memory");
+      if (m < M) {
 #pragma unroll
-      for (int r = 0; r < 4; r++) {
-        const int m = m0 + wm + 16 * i + g + (r >= 2 ? 8 : 0);
-        const int n = n0 + wn + 8 * j + 2 * t + (r & 1);
-        if (m < M && n < N) {
-          float v = alpha * acc[i][j][r];
-          if (epi != EPI_NONE) v += bias[n];
-          if (epi == EPI_BIAS_TANH) v = tanhf(v);
-          Cm[m * ldc + n] = v;
+        for (int j = 0; j < 32; j++) {
+          const int n = n0 + 32 * half + j;
+          if (n < N) {
+            float x = alpha * __uint_as_float(v[j]);
+            if (epi != EPI_NONE) x += bias[n];
+            if (epi == EPI_BIAS_TANH) x = tanhf(x);
+            Cm[m * ldc + n] = x;
+          }
         }
       }
+    }
+  } else {
+    // a wait gave up: record it, let the products in flight finish (again
+    // bounded) before the tensor memory is released
+    if (tid == 0) atomicExch(err, 1);
+    mbar_wait(mb, (uint32_t)((nchunks - 1) & 1));
+  }
+  asm volatile("tcgen05.fence::before_thread_sync;\n" ::: "memory");
+  __syncthreads();
+  if (warp == 0) {
+    asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory");
+    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;\n" ::"r"(tmem), "n"(TC_TMEM_COLS) : "memory");
+  }
 }
+
+int* g_tc_err = nullptr;  // set by k_gemm_tc when a bounded wait gave up
 
 void gemm(int M, int N, int K, const float* A, long long sam, long long sak, const float* B, long long sbk,
           long long sbn, float* C, long long ldc, const float* bias, int epi, float alpha = 1.f) {
-  dim3 grid((N + GT - 1) / GT, (M + GT - 1) / GT);
-  NRPYELL_LAUNCH(k_gemm_bf16, grid, 128, 0, M, N, K, A, sam, sak, B, sbk, sbn, C, ldc, bias, epi, alpha);
+  static unsigned long long opted = 0;
+  int dev = 0;
+  NRPYELL_CUDA(cudaGetDevice(&dev));
+  if (dev >= 0 && dev < 64 && !(opted >> dev & 1ull)) {
+    NRPYELL_CUDA(cudaFuncSetAttribute(k_gemm_tc, cudaFuncAttributeMaxDynamicSharedMemorySize, TC_SMEM));
+    opted |= 1ull << dev;
+  }
+  if (!g_tc_err) {
+    NRPYELL_CUDA(dev_alloc(&g_tc_err, sizeof(int)));
+    NRPYELL_CUDA(cudaMemset(g_tc_err, 0, sizeof(int)));
+  }
+  if (M <= 0 || N <= 0 || K <= 0) {
+    NRPYELL_FAIL("k_gemm_tc: empty matrix product");
+    return;
+  }
+  dim3 grid((N + TC_N - 1) / TC_N, (M + TC_M - 1) / TC_M);
+  NRPYELL_LAUNCH(k_gemm_tc, grid, 128, TC_SMEM, M, N, K, A, sam, sak, B, sbk, sbn, C, ldc, bias, epi, alpha, g_tc_err);
+}
+
+// Reports (once) a bounded wait of the tensor-core GEMM that gave up.
+bool gemm_ok() {
+  if (!g_tc_err) return true;
+  int e = 0;
+  NRPYELL_CUDA(cudaMemcpy(&e, g_tc_err, sizeof(int), cudaMemcpyDeviceToHost));
+  if (e) {
+    NRPYELL_CUDA(cudaMemset(g_tc_err, 0, sizeof(int)));
+    NRPYELL_FAIL("k_gemm_tc: a bounded wait for the tensor-core products gave up");
+    return false;
+  }
+  return status_ok();
 }
 
 // ------------------------------------------------------ elementwise pieces
@@ -373,7 +493,7 @@ int nrpyell_mlp_predict(void* mlp, const float* x, int n, float* y) {
                                  cudaMemcpyDeviceToDevice, stream()));
   }
   NRPYELL_CUDA(cudaStreamSynchronize(stream()));
-  return status_ok() ? 0 : -1;
+  return gemm_ok() ? 0 : -1;
 }
 
 double nrpyell_mlp_loss_grad(void* mlp, const float* x, const float* t, int rows, float* grad_host) {
@@ -390,6 +510,7 @@ double nrpyell_mlp_loss_grad(void* mlp, const float* x, const float* t, int rows
   if (grad_host)
     NRPYELL_CUDA(cudaMemcpyAsync(grad_host, q->grad, sizeof(float) * q->n_params, cudaMemcpyDeviceToHost, stream()));
   NRPYELL_CUDA(cudaStreamSynchronize(stream()));
+  if (!gemm_ok()) return NAN;
   return loss / ((double)rows * q->n_out);
 }
 
@@ -433,6 +554,7 @@ double nrpyell_mlp_train(void* mlp, const float* x, const float* t, int n, int b
     double sum = 0.0;
     NRPYELL_CUDA(cudaMemcpyAsync(&sum, q->loss, sizeof(double), cudaMemcpyDeviceToHost, stream()));
     NRPYELL_CUDA(cudaStreamSynchronize(stream()));
+    if (!gemm_ok()) return NAN;
     last = sum / ((double)per_epoch * batch * q->n_out);
     if (loss_history) loss_history[e] = last;
   }
