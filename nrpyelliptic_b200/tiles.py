@@ -2,6 +2,12 @@
 configuration's grid -- the table the autotuner chooses from.
 
     python -m nrpyelliptic_b200.tiles [CONFIG ...] [--launches N] [--tile T]
+    python -m nrpyelliptic_b200.tiles [CONFIG ...] --mixed STEPS
+
+--mixed runs STEPS RK4 steps of the mixed-precision driver's FP32 correction
+form from the zero guess instead (after a warm-up of the same length) and
+prints the time per step: the launch to capture when profiling the FP32
+correction kernels.
 
 For each shape: the stage-1, stage-2 and stage-4 kernels (CUDA-event time
 averaged over N launches replayed from a CUDA graph) and one whole RK4 step,
@@ -56,12 +62,45 @@ def sweep(name, launches=50, lib=None, only=None):
     return rows
 
 
+def mixed_steps(name, steps, lib=None, tile=None):
+    """Microseconds per RK4 step of the FP32 correction form (nrpyell_relax_mixed
+    with every step in FP32, folds every 256 steps) over `steps` steps."""
+    import time
+    lib = lib or _lib.load()
+    prob = Problem(CONFIGS[name], lib=lib)
+    ds = DeviceState(prob)
+    n32, n64, fin = C.c_int(), C.c_int(), C.c_double()
+    if tile is not None:
+        lib.nrpyell_set_tile(tile)
+    out = []
+    for _ in range(2):  # warm-up (autotuning, graph capture), then timed
+        lib.nrpyell_memset(ds.ptr["y_n"], 0, 2 * prob.Ntot * 8)
+        lib.nrpyell_synchronize()
+        t0 = time.perf_counter()
+        lib.nrpyell_relax_mixed(C.byref(ds.g), prob.dt, -30.0, -30.0, 256, steps, prob.cfg.R_L2, C.byref(n32),
+                                C.byref(n64), C.byref(fin), None)
+        lib.nrpyell_synchronize()
+        out.append((time.perf_counter() - t0) * 1e6 / max(1, n32.value))
+        _lib.check(lib)
+    tile = lib.nrpyell_get_tile(C.byref(prob.params), 2, None, None, None)
+    lib.nrpyell_set_tile(-1)
+    ds.free()
+    return out[-1], n32.value, tile
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("configs", nargs="*", default=["quasicircular_128x128x16", "unequal_spinning_256x256x32"])
     ap.add_argument("--launches", type=int, default=50)
     ap.add_argument("--tile", type=int, default=None, help="time this tile shape only")
+    ap.add_argument("--mixed", type=int, default=0, help="time STEPS steps of the FP32 correction form instead")
     args = ap.parse_args()
+    if args.mixed:
+        for name in args.configs:
+            us, n, tile = mixed_steps(name, args.mixed, tile=args.tile)
+            print("%s: FP32 correction form, %d steps, %.2f us per RK4 step (wall clock, folds included), tile %d"
+                  % (name, n, us, tile))
+        return
     for name in args.configs:
         print("| %s | tile | 32 x by x planes | kind | stage 1 us | stage 2 us | stage 2 GB/s | stage 4 us | RK4 step us |"
               % name)
