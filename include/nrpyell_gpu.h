@@ -137,7 +137,7 @@ void nrpyell_set_async(int enable);
  * nrpyell_get_tile reports the shape in use for a grid (block 32 x by threads,
  * `planes` consecutive i2 planes per thread), -1 if not tuned yet; its fp32
  * argument selects FP64 (0), FP32 (1) or the FP32 correction form of
- * nrpyell_relax_mixed (2, marching shapes only).
+ * nrpyell_relax_mixed (2: marching shapes and the 8-warp direct shapes).
  * nrpyell_num_tiles gives the number of shapes; nrpyell_tile_info describes
  * shape t and returns -1 for an index out of range.  kind: 0 one thread per
  * (i0,i1) column of `planes` points reading its stencil through L1; 2 the

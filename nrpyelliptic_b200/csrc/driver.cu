@@ -130,10 +130,10 @@ SubstepArgs substep_args(const Dims& d, RfmTables* rt, BcTables* bt, Scratch* s,
 template <typename T>
 int tuned_tile(const Dims& d, RfmTables* rt, BcTables* bt, FusedWork* w, Scratch* sc, const StateBuffers& b,
                const RelaxParams& rp) {
-  // the correction form runs on the marching shapes only
+  // the correction form runs on the marching and 8-warp direct shapes
   const bool corr = b.R0 != nullptr;
   const int which = sizeof(T) == 8 ? 0 : (corr ? 2 : 1);
-  if (g_forced_tile >= 0 && !(corr && substep_tile_kind(g_forced_tile) != 5)) return g_forced_tile;
+  if (g_forced_tile >= 0 && !(corr && !substep_supports_correction(g_forced_tile))) return g_forced_tile;
   if (w->tile[which] >= 0) return w->tile[which];
   cudaEvent_t e0, e1;
   NRPYELL_CUDA(cudaEventCreate(&e0));
@@ -145,7 +145,7 @@ int tuned_tile(const Dims& d, RfmTables* rt, BcTables* bt, FusedWork* w, Scratch
   // would write y_n, the caller's state, so it is left out -- stages 1-3
   // write only the running total and the stage buffers.
   for (int t = 0; t < substep_num_tiles(); t++) {
-    if (corr && (substep_tile_kind(t) != 5 || !march_fits(d))) continue;
+    if (corr && (!substep_supports_correction(t) || !march_fits(d))) continue;
     SubstepArgs a[3];
     for (int st = 1; st <= 3; st++) a[st - 1] = substep_args(d, rt, bt, sc, b, rp, st, w->zero_flag, w->state, t);
     prepare_substep<T>(t);

@@ -69,6 +69,8 @@ void launch_ghost_fill(const Dims& d, const BcTables* bt, void* gfs);
 int substep_num_tiles();
 void substep_tile_shape(int tile, int* bx, int* by, int* p);
 int substep_tile_kind(int tile);  // see nrpyell_tile_info
+// Shapes that run the correction form (SubstepArgs::R0).
+bool substep_supports_correction(int tile);
 int substep_interior_blocks(const Dims& d, int tile);
 // One-time per-shape setup (shared-memory opt-in); call before a stream
 // capture that launches the shape.

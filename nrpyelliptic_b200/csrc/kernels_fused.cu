@@ -34,20 +34,23 @@
 namespace nrpyell {
 
 // ------------------------------------------------------- direct interior
-template <typename T, int STAGE, bool RESID, int BY, int P, bool PF>
+// CORR: the correction form of the mixed-precision driver
+// (point_rhs_correction; 8-warp shapes without PF only).
+template <typename T, int STAGE, bool RESID, int BY, int P, bool PF, bool CORR = false>
 __global__ void __launch_bounds__(32 * BY) k_substep(SubDev<T> a) {
   constexpr int NT = 32 * BY;
+  static_assert(!CORR || (NT >= 256 && !PF), "the correction form runs on 8-warp shapes without PF");
   __shared__ double sh[NT / 32 > 8 ? NT / 32 : 8];
   // radiation columns: blocks of 256 threads take 32 columns by rows
   // (column_rows), narrower blocks 16 threads per column (column_block)
   constexpr bool ROWS = NT >= 256;
-  __shared__ double csm[ROWS ? kRowsSmem : 1];
+  __shared__ double csm[ROWS ? (CORR ? kRowsSmemCorr : kRowsSmem) : 1];
   __shared__ bool last;
   pdl_enter();
   if (*a.done) return;
   if ((int)blockIdx.x < a.n_col_blocks) {
     if constexpr (ROWS)
-      column_rows<T, STAGE, NT>(a, blockIdx.x, csm);
+      column_rows<T, STAGE, NT, CORR>(a, blockIdx.x, csm);
     else
       column_block<T, STAGE, NT>(a, blockIdx.x);
     return;
@@ -134,6 +137,16 @@ __global__ void __launch_bounds__(32 * BY) k_substep(SubDev<T> a) {
           yv = pf[5][p];
           accu = pf[6][p];
           accv = pf[7][p];
+        } else if (CORR) {
+          T ju, jv;
+          point_rhs_correction<T>(col[p + 5], __ldg(a.S + (idx + Ntot)), __ldg(a.aux + (idx + ADD_TIMES_AUUGF * Ntot)),
+                                  __ldg(a.aux + (idx + PSI_BACKGROUNDGF * Ntot)),
+                                  __ldg(a.aux + (idx + WAVESPEEDGF * Ntot)), C22, C00, C11, C1, C0, Cc, s0, s1, s00,
+                                  s11, s22, a.eta, __ldg(a.R0 + idx), __ldg(a.R0 + (idx + Ntot)), ku, kv, br, ju, jv);
+          accu = (STAGE == 1) ? (T)0 : a.acc[idx];
+          accv = (STAGE == 1) ? (T)0 : a.acc[idx + Ntot];
+          yu = y_is_s ? col[p + 5] : a.y[idx];
+          yv = y_is_s ? __ldg(a.S + (idx + Ntot)) : a.y[idx + Ntot];
         } else {
           point_rhs<T>(col[p + 5], __ldg(a.S + (idx + Ntot)), __ldg(a.aux + (idx + ADD_TIMES_AUUGF * Ntot)),
                        __ldg(a.aux + (idx + PSI_BACKGROUNDGF * Ntot)), __ldg(a.aux + (idx + WAVESPEEDGF * Ntot)), C22,
@@ -394,9 +407,13 @@ int substep_interior_blocks(const Dims& d, int tile) {
 template <typename T, int STAGE, bool RESID, int BY, int P>
 static void launch_planes(const SubstepArgs& a);
 
-template <typename T, int STAGE, bool RESID, int BY, int P, bool PF>
+template <typename T, int STAGE, bool RESID, int BY, int P, bool PF, bool CORR = false>
 static void launch_direct(const SubstepArgs& a) {
   if (!march_fits(a.d)) {  // 64-bit offsets: the planes kernel
+    if (CORR) {
+      NRPYELL_FAIL("launch_direct: the correction form needs 3 Ntot < 2^32");
+      return;
+    }
     launch_planes<T, STAGE, RESID, 8, 1>(a);
     return;
   }
@@ -404,7 +421,7 @@ static void launch_direct(const SubstepArgs& a) {
   constexpr int NT = 32 * BY;
   constexpr int CB = NT / kColThreadsPerColumn;
   f.n_col_blocks = NT >= 256 ? ((a.d.Nxx1 + kRows - 1) / kRows) * a.d.Nxx2 : (f.ncol + CB - 1) / CB;
-  NRPYELL_LAUNCH_PDL((k_substep<T, STAGE, RESID, BY, P, PF>), f.n_tiles + f.n_col_blocks, NT, 0, f);
+  NRPYELL_LAUNCH_PDL((k_substep<T, STAGE, RESID, BY, P, PF, CORR>), f.n_tiles + f.n_col_blocks, NT, 0, f);
 }
 
 template <typename T, int STAGE, bool RESID, int BY, int P>
@@ -544,13 +561,43 @@ static void launch_tile(const SubstepArgs& a) {
   }
 }
 
+// Shapes that run the correction form: the marching shapes and the 8-warp
+// direct shapes without prefetch (32 x 8 x 1, 32 x 8 x 2).
+bool substep_supports_correction(int tile) {
+  return tile >= 0 && tile < kNumTiles && (kTiles[tile].kind == 5 || tile == 3 || tile == 4);
+}
+
+template <typename T, int STAGE, bool RESID>
+static void launch_direct_correction(const SubstepArgs& a) {
+  if constexpr (sizeof(T) == 4) {
+    if (a.tile == 3)
+      launch_direct<T, STAGE, RESID, 8, 1, false, true>(a);
+    else
+      launch_direct<T, STAGE, RESID, 8, 2, false, true>(a);
+  }
+}
+
 template <typename T>
 void launch_substep(int stage, const SubstepArgs& a) {
-  if (a.R0 && (sizeof(T) != 4 || kTiles[a.tile].kind != 5)) {
-    NRPYELL_FAIL("launch_substep: the correction form runs on FP32 marching shapes only");
+  if (a.R0 && (sizeof(T) != 4 || !substep_supports_correction(a.tile))) {
+    NRPYELL_FAIL("launch_substep: the correction form runs on FP32 marching and 8-warp direct shapes only");
     return;
   }
   const bool resid = (stage == 1) && a.lt;
+  if (a.R0 && kTiles[a.tile].kind != 5) {
+    switch (stage) {
+      case 1:
+        if (resid)
+          launch_direct_correction<T, 1, true>(a);
+        else
+          launch_direct_correction<T, 1, false>(a);
+        break;
+      case 2: launch_direct_correction<T, 2, false>(a); break;
+      case 3: launch_direct_correction<T, 3, false>(a); break;
+      default: launch_direct_correction<T, 4, false>(a); break;
+    }
+    return;
+  }
   switch (stage) {
     case 1:
       if (resid)

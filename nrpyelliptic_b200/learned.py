@@ -6,6 +6,7 @@ the zero guess's (else the zero guess is the fallback), and the FP64
 relaxation from either start decides the final error.
 
     python -m nrpyelliptic_b200.learned [--train 4096] [--test 256] [--modes 256] [--epochs 400]
+    python -m nrpyelliptic_b200.learned --mlp-only [--epochs 5]   (network training throughput)
 
 Pipeline (one GPU):
   1. training solves: `--train` configurations drawn from the seeded sweep
@@ -332,6 +333,34 @@ def report(ev, print=print):
           % (ev["err_learned"].max(), ev["err_mixed"].max()))
 
 
+def mlp_throughput(lib, n=4096, epochs=5, width=512, depth=4, n_out=256, batch=256):
+    """Training throughput of the network alone (the learned guess's shape,
+    13 -> depth x width -> n_out, minibatch `batch`) on seeded synthetic
+    data: seconds per epoch and the matrix-product TFLOP/s (forward and both
+    backward products: 6 flops per weight per row)."""
+    rng = np.random.default_rng(3)
+    x = rng.normal(size=(n, N_FEATURES)).astype(np.float32)
+    t = rng.normal(size=(n, n_out)).astype(np.float32)
+    mlp = lib.nrpyell_mlp_create(N_FEATURES, width, depth, n_out, batch, 1)
+    dx = lib.nrpyell_device_malloc(x.nbytes)
+    dt = lib.nrpyell_device_malloc(t.nbytes)
+    lib.nrpyell_memcpy(dx, x.ctypes.data, x.nbytes, 0)
+    lib.nrpyell_memcpy(dt, t.ctypes.data, t.nbytes, 0)
+    lib.nrpyell_mlp_train(mlp, dx, dt, n, batch, 1, 1e-3, 1, None)  # warm-up
+    lib.nrpyell_synchronize()
+    t0 = time.perf_counter()
+    lib.nrpyell_mlp_train(mlp, dx, dt, n, batch, epochs, 1e-3, 1, None)
+    lib.nrpyell_synchronize()
+    sec = (time.perf_counter() - t0) / epochs
+    _lib.check(lib)
+    weights = N_FEATURES * width + (depth - 1) * width * width + width * n_out
+    flops = 6.0 * weights * (n // batch) * batch
+    lib.nrpyell_device_free(dx)
+    lib.nrpyell_device_free(dt)
+    lib.nrpyell_mlp_destroy(mlp)
+    return sec, flops / sec / 1e12
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--train", type=int, default=4096)
@@ -341,8 +370,15 @@ def main():
     ap.add_argument("--seed", type=int, default=20261203)
     ap.add_argument("--test-seed", type=int, default=20261204)
     ap.add_argument("--dump", default=None, help="write the regression data (features, POD coefficients) to this .npz")
+    ap.add_argument("--mlp-only", action="store_true",
+                    help="time the network's training on synthetic data only (no solves)")
     args = ap.parse_args()
     lib = _lib.load()
+    if args.mlp_only:
+        sec, tflops = mlp_throughput(lib, epochs=args.epochs)
+        print("MLP 13 -> 4 x 512 -> 256, minibatch 256, 4096 rows: %.2f ms per epoch, %.2f TFLOP/s in the matrix "
+              "products" % (sec * 1e3, tflops))
+        return
     T = {}
     t = time.perf_counter()
     train_cfgs = configs(args.train, args.seed)

@@ -98,16 +98,16 @@ def test_every_tile_relaxes_to_the_same_solution(lib):
         lib.nrpyell_set_tile(-1)
 
 
-def test_marching_tiles_in_mixed_precision(lib):
-    """The FP32 correction form of the mixed-precision driver on every
-    marching shape (the only kind that runs it)."""
+def test_correction_form_tiles_in_mixed_precision(lib):
+    """The FP32 correction form of the mixed-precision driver on every shape
+    that runs it: the marching shapes and the 8-warp direct shapes."""
     gold = load_golden("relax_shipped_64x64x8.npz")
     prob = Problem(CONFIGS["shipped_64x64x8"])
     N = prob.N
     ref = gold["uu_interior"]
     try:
         for t, by, p, kind in tiles(lib):
-            if kind != 5:
+            if not (kind == 5 or (kind == 0 and by == 8)):
                 continue
             lib.nrpyell_set_tile(t)
             ds = DeviceState(prob)
