@@ -107,7 +107,7 @@ def measured_hbm_peak():
 
 
 # Fused substep kernel of each tile kind (nrpyell_tile_info).
-KERNELS = {0: "k_substep", 2: "k_substep", 3: "k_substep_bulk", 4: "k_substep_planes", 5: "k_substep_march"}
+KERNELS = {0: "k_substep", 2: "k_substep", 4: "k_substep_planes", 5: "k_substep_march"}
 
 
 def profiled_traffic(kernel, tag):

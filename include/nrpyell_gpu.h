@@ -141,10 +141,8 @@ void nrpyell_set_async(int enable);
  * nrpyell_num_tiles gives the number of shapes; nrpyell_tile_info describes
  * shape t and returns -1 for an index out of range.  kind: 0 one thread per
  * (i0,i1) column of `planes` points reading its stencil through L1; 2 the
- * same with the pointwise inputs loaded before the first store; 3 TMA
- * pipeline (persistent CTAs, tiles staged by tensor-map bulk copies, FP64
- * only -- FP32 runs shape kind 2 instead); 4 the block's uu planes staged in
- * shared memory; 5 the block marches through `planes` i2 planes, each plane
+ * same with the pointwise inputs loaded before the first store; 4 the
+ * block's uu planes staged in shared memory; 5 the block marches through `planes` i2 planes, each plane
  * and its pointwise inputs copied into shared memory ahead of use by
  * asynchronous copies. */
 void nrpyell_set_tile(int tile);

@@ -18,9 +18,8 @@ CSRC = os.path.join(HERE, "csrc")
 INCLUDE = os.path.join(ROOT, "include")
 LIB = os.path.join(HERE, "libnrpyell_gpu.so")
 
-SOURCES = ["capi.cu", "driver.cu", "batch.cu", "tables.cu", "tables_gpu.cu", "kernels_ref.cu", "kernels_fused.cu", "kernels_march.cu",
-           "kernels_bulk.cu",
-           "noalloc.cu", "mlp.cu", "setup_gpu.cu", "export.cu",
+SOURCES = ["capi.cu", "driver.cu", "batch.cu", "tables.cu", "tables_gpu.cu", "kernels_ref.cu", "kernels_fused.cu",
+           "kernels_march.cu", "noalloc.cu", "mlp.cu", "setup_gpu.cu", "export.cu",
            "setup.cpp"]
 OBJDIR = os.path.join(HERE, "_build")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]

@@ -305,7 +305,7 @@ RelaxResult relax_loop(const Dims& d, RfmTables* rt, BcTables* bt, L2Tables* lt,
   if (!status_ok()) return res;
   if (st[5]) {
     char msg[128];
-    snprintf(msg, sizeof(msg), "fused substep: a bounded wait of the bulk-copy pipeline gave up (code %d)", st[5]);
+    snprintf(msg, sizeof(msg), "fused substep: a bounded wait of a substep kernel gave up (code %d)", st[5]);
     NRPYELL_FAIL(msg);
     return res;
   }

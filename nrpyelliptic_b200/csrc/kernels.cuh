@@ -77,12 +77,8 @@ int substep_interior_blocks(const Dims& d, int tile);
 template <typename T>
 void prepare_substep(int tile);
 
-// Radiation-BC columns of a substep as their own kernel on side_stream(),
-// forked from stream(); join_columns() makes stream() wait for them.
-// prepare_columns() creates the stream and events (before a capture).
-template <typename T>
-void launch_columns_forked(int stage, const SubstepArgs& a);
-void join_columns();
+// Side stream and events of the stop test (launch_finalize_forked); call
+// before a stream capture.
 void prepare_columns();
 
 // Stop test of a stage-1 launch made with defer_l2 = 1: one block on
@@ -106,11 +102,5 @@ void prepare_march(int v);
 // Interior blocks of shape v's launch on this grid (its split of the planes).
 template <typename T>
 int march_interior_blocks(int v, const SubstepArgs& a);
-
-// ---- bulk-copy pipeline variant (kernels_bulk.cu), FP64 ----
-// Usable when the row length N0 is even and every array is 16-byte aligned.
-bool bulk_available(const SubstepArgs& a, size_t elem_size);
-void launch_bulk(int stage, int shape, const SubstepArgs& a);
-void prepare_bulk(int shape);
 
 }  // namespace nrpyell

@@ -24,9 +24,8 @@
 // consecutive i2 planes, holds uu along i2 in registers and reads the rest of
 // its 31-point star through L1 (optionally loading the pointwise inputs of
 // all P planes before the first store), and the shared-memory planes
-// variant.  kernels_march.cu holds the marching variant and kernels_bulk.cu
-// the bulk-copy pipeline variant; the autotuner picks among the shapes of
-// all of them (the tile table below).
+// variant.  kernels_march.cu holds the marching variant; the autotuner picks
+// among the shapes of all of them (the tile table below).
 // The metric factors of the RHS depend on (i0,i1) only and are folded into
 // six per-(i0,i1) weights (tables.cu), leaving one division per point.
 #include "substep.cuh"
@@ -174,13 +173,6 @@ __global__ void __launch_bounds__(32 * BY) k_substep(SubDev<T> a) {
     }
   }
   if (RESID && tile_partial<NT>(r2, b, a.partials, a.ticket, a.n_tiles, sh, &last, a.defer_l2 != 0)) finalize_l2<T, NT>(a, sh);
-}
-
-template <typename T, int STAGE>
-__global__ void __launch_bounds__(128) k_radiation_rows(SubDev<T> a) {
-  __shared__ double smem[kRowsSmem];
-  if (*a.done) return;
-  column_rows<T, STAGE, 128>(a, blockIdx.x, smem);
 }
 
 // ------------------------------------------------- planes in shared memory
@@ -372,18 +364,16 @@ __global__ void k_ghost_fill(const int2* __restrict__ map, const signed char* __
 // ------------------------------------------------------------------ tiles
 
 // kind 0: direct; 2: direct with the pointwise inputs of all P planes loaded
-// up front; 3: TMA pipeline (kernels_bulk.cu) shape v, FP64 on grids with an
-// even row length and 16-byte aligned arrays, else kind 2 (4, 2); 4: planes
-// in shared memory (its column blocks by rows, column_rows); 5: marching
-// along i2 with asynchronous copies (kernels_march.cu), p planes per block,
-// v the index of its compiled shape there.
+// up front; 4: planes in shared memory (its column blocks by rows,
+// column_rows); 5: marching along i2 with asynchronous copies
+// (kernels_march.cu), p planes per block, v the index of its compiled shape
+// there.
 struct TileShape {
   int by, p, kind, v;
 };
 static const TileShape kTiles[] = {{4, 1, 0, 0}, {4, 2, 0, 0}, {2, 4, 0, 0}, {8, 1, 0, 0}, {8, 2, 0, 0},
                                    {4, 4, 0, 0}, {4, 1, 2, 0}, {4, 2, 2, 0}, {2, 4, 2, 0}, {4, 4, 2, 0},
-                                   {8, 2, 2, 0}, {4, 4, 3, 0}, {4, 4, 3, 1}, {8, 2, 3, 2}, {2, 8, 3, 3},
-                                   {4, 2, 3, 4}, {4, 2, 4, 0}, {4, 4, 4, 0}, {8, 2, 4, 0}, {2, 4, 4, 0},
+                                   {8, 2, 2, 0}, {4, 2, 4, 0}, {4, 4, 4, 0}, {8, 2, 4, 0}, {2, 4, 4, 0},
                                    {8, 1, 4, 0}, {4, 1, 4, 0}, {8, 4, 4, 0}, {8, 8, 5, 0}, {8, 16, 5, 1},
                                    {8, 4, 5, 2}, {8, 4, 5, 3}, {8, 8, 5, 4}, {8, 32, 5, 5}, {8, 4, 5, 6}};
 constexpr int kNumTiles = sizeof(kTiles) / sizeof(kTiles[0]);
@@ -432,40 +422,14 @@ static void launch_planes(const SubstepArgs& a) {
   NRPYELL_LAUNCH_PDL((k_substep_planes<T, STAGE, RESID, BY, P>), f.n_tiles + f.n_col_blocks, NT, 0, f);
 }
 
-static cudaEvent_t g_fork = nullptr, g_join = nullptr, g_fin_fork = nullptr, g_fin_join = nullptr;
+static cudaEvent_t g_fin_fork = nullptr, g_fin_join = nullptr;
 
 void prepare_columns() {
   side_stream();
-  if (!g_fork) {
-    NRPYELL_CUDA(cudaEventCreateWithFlags(&g_fork, cudaEventDisableTiming));
-    NRPYELL_CUDA(cudaEventCreateWithFlags(&g_join, cudaEventDisableTiming));
+  if (!g_fin_fork) {
     NRPYELL_CUDA(cudaEventCreateWithFlags(&g_fin_fork, cudaEventDisableTiming));
     NRPYELL_CUDA(cudaEventCreateWithFlags(&g_fin_join, cudaEventDisableTiming));
   }
-}
-
-template <typename T>
-void launch_columns_forked(int stage, const SubstepArgs& a) {
-  prepare_columns();
-  SubDev<T> f = make_dev<T>(a, 4, 1);
-  f.n_col_blocks = 0;
-  const int grid = ((a.d.Nxx1 + kRows - 1) / kRows) * a.d.Nxx2;
-  cudaStream_t side = side_stream();
-  NRPYELL_CUDA(cudaEventRecord(g_fork, stream()));
-  NRPYELL_CUDA(cudaStreamWaitEvent(side, g_fork, 0));
-  switch (stage) {
-    case 1: NRPYELL_LAUNCH_ON(side, (k_radiation_rows<T, 1>), grid, 128, 0, f); break;
-    case 2: NRPYELL_LAUNCH_ON(side, (k_radiation_rows<T, 2>), grid, 128, 0, f); break;
-    case 3: NRPYELL_LAUNCH_ON(side, (k_radiation_rows<T, 3>), grid, 128, 0, f); break;
-    default: NRPYELL_LAUNCH_ON(side, (k_radiation_rows<T, 4>), grid, 128, 0, f); break;
-  }
-}
-template void launch_columns_forked<double>(int, const SubstepArgs&);
-template void launch_columns_forked<float>(int, const SubstepArgs&);
-
-void join_columns() {
-  NRPYELL_CUDA(cudaEventRecord(g_join, side_stream()));
-  NRPYELL_CUDA(cudaStreamWaitEvent(stream(), g_join, 0));
 }
 
 // The stop test of a deferred stage-1 launch (tile_partial with defer): one
@@ -480,18 +444,13 @@ __global__ void __launch_bounds__(256) k_finalize_l2(SubDev<T> a) {
 template <typename T>
 void launch_finalize_forked(const SubstepArgs& a1) {
   prepare_columns();
-  // the tile grid of the stage-1 launch, as launch_tile chose it: kind 3 runs
-  // the direct 32x4x2 shape where the bulk pipeline is unavailable, and the
-  // 32-bit-offset kernels (direct, marching) the planes 32x8x1 shape on grids
-  // too large for them
+  // the tile grid of the stage-1 launch, as launch_tile chose it: the
+  // 32-bit-offset kernels (direct, marching) run the planes 32x8x1 shape on
+  // grids too large for them
   const TileShape s = kTiles[a1.tile];
   const bool fits = march_fits(a1.d);
   int by = s.by, p = s.p;
-  if (s.kind == 3 && !bulk_available(a1, sizeof(T))) {
-    by = 4;
-    p = 2;
-  }
-  if (!fits && s.kind != 4 && !(s.kind == 3 && bulk_available(a1, sizeof(T)))) {
+  if (!fits && s.kind != 4) {
     by = 8;
     p = 1;
   }
@@ -510,9 +469,8 @@ void join_finalize() { NRPYELL_CUDA(cudaStreamWaitEvent(stream(), g_fin_join, 0)
 
 template <typename T>
 void prepare_substep(int tile) {
-  if (kTiles[tile].kind == 3) prepare_bulk(kTiles[tile].v);
   if (kTiles[tile].kind == 5) prepare_march<T>(kTiles[tile].v);
-  if (kTiles[tile].kind == 3 || kTiles[tile].kind == 5) prepare_columns();  // side stream and events
+  prepare_columns();  // side stream and events of the stop test
 }
 template void prepare_substep<double>(int);
 template void prepare_substep<float>(int);
@@ -531,30 +489,20 @@ static void launch_tile(const SubstepArgs& a) {
     case 8: launch_direct<T, STAGE, RESID, 2, 4, true>(a); break;
     case 9: launch_direct<T, STAGE, RESID, 4, 4, true>(a); break;
     case 10: launch_direct<T, STAGE, RESID, 8, 2, true>(a); break;
-    case 11:
-    case 12:
-    case 13:
-    case 14:
-    case 15:
-      if (bulk_available(a, sizeof(T)))
-        launch_bulk(STAGE, kTiles[a.tile].v, a);
-      else
-        launch_direct<T, STAGE, RESID, 4, 2, true>(a);
-      break;
-    case 16: launch_planes<T, STAGE, RESID, 4, 2>(a); break;
-    case 17: launch_planes<T, STAGE, RESID, 4, 4>(a); break;
-    case 18: launch_planes<T, STAGE, RESID, 8, 2>(a); break;
-    case 19: launch_planes<T, STAGE, RESID, 2, 4>(a); break;
-    case 20: launch_planes<T, STAGE, RESID, 8, 1>(a); break;
-    case 21: launch_planes<T, STAGE, RESID, 4, 1>(a); break;
-    case 22: launch_planes<T, STAGE, RESID, 8, 4>(a); break;
+    case 11: launch_planes<T, STAGE, RESID, 4, 2>(a); break;
+    case 12: launch_planes<T, STAGE, RESID, 4, 4>(a); break;
+    case 13: launch_planes<T, STAGE, RESID, 8, 2>(a); break;
+    case 14: launch_planes<T, STAGE, RESID, 2, 4>(a); break;
+    case 15: launch_planes<T, STAGE, RESID, 8, 1>(a); break;
+    case 16: launch_planes<T, STAGE, RESID, 4, 1>(a); break;
+    case 17: launch_planes<T, STAGE, RESID, 8, 4>(a); break;
+    case 18:
+    case 19:
+    case 20:
+    case 21:
+    case 22:
     case 23:
     case 24:
-    case 25:
-    case 26:
-    case 27:
-    case 28:
-    case 29:
       if (!launch_march<T>(STAGE, RESID, kTiles[a.tile].v, a)) launch_planes<T, STAGE, RESID, 8, 1>(a);
       break;
     default: NRPYELL_FAIL("launch_substep: tile index out of range"); break;

@@ -1,8 +1,7 @@
 // Device code shared by the fused RK4 substep kernels (kernels_fused.cu: one
 // thread per (i0,i1) column of P points reading through L1, or the block's
 // planes staged in shared memory; kernels_march.cu: blocks marching along i2
-// with the planes copied ahead by cp.async; kernels_bulk.cu: tiles staged in
-// shared memory by bulk asynchronous copies): the launch arguments, the point
+// with the planes copied ahead by cp.async): the launch arguments, the point
 // RHS, the RK combination, the radiation-BC column work and the stop-test
 // reduction.  Every variant evaluates a point with the same
 // operations in the same order, so all of them produce identical bits.
@@ -215,14 +214,9 @@ __device__ __forceinline__ void store_point(const SubDev<T>& a, long long idx, T
   a.out[a.Ntot + idx] = ov;
 }
 
-// Barrier over the NT threads that reduce: the whole block, or (bulk kernel)
-// the consumer warps only, on a named barrier.
+// Barrier over the NT threads that reduce (the whole block).
 struct BlockSync {
   static __device__ __forceinline__ void sync() { __syncthreads(); }
-};
-template <int ID, int NT>
-struct NamedSync {
-  static __device__ __forceinline__ void sync() { asm volatile("bar.sync %0, %1;\n" ::"n"(ID), "n"(NT) : "memory"); }
 };
 
 // Stop test: the block that completes the last tile sums the per-tile
@@ -436,9 +430,8 @@ __device__ void column_block(const SubDev<T>& a, int cb) {
 }
 
 // ------------------------------------------------ radiation columns by rows
-// The radiation BC of the x0max face: the column blocks of the shared-memory
-// planes kernel, and a kernel of its own that runs beside the persistent TMA
-// pipeline kernel on the side stream.  A block takes
+// The radiation BC of the x0max face: the column blocks of the 8-warp
+// direct, shared-memory planes and marching kernels.  A block takes
 // kRows consecutive i1 columns at one i2: it copies the outer 12 points of
 // uu and vv along i0 on those rows and on 5 rows either side (rows across
 // the axis from their images) into shared memory, then computes every

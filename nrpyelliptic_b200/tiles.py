@@ -22,7 +22,7 @@ from . import _lib
 from .problem import CONFIGS, DeviceState, Problem
 
 STAGE2_BYTES = 104
-KINDS = {0: "direct", 2: "direct+prefetch", 3: "tma pipeline", 4: "smem planes", 5: "smem march"}
+KINDS = {0: "direct", 2: "direct+prefetch", 4: "smem planes", 5: "smem march"}
 
 
 def shapes(lib):

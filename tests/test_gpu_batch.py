@@ -13,8 +13,8 @@ from nrpyelliptic_b200.batch import relax_batch
 from nrpyelliptic_b200.problem import CONFIGS, DeviceState, Problem, sample_sweep, with_grid
 
 pytestmark = pytest.mark.gpu
-PLANES_8x1 = 20  # a shared-memory planes tile shape (kind 4)
-MARCH_8x4 = 25  # a marching tile shape (kind 5)
+PLANES_8x1 = 15  # a shared-memory planes tile shape (kind 4)
+MARCH_8x4 = 20  # a marching tile shape (kind 5)
 
 
 @pytest.fixture(scope="module")

@@ -11,7 +11,7 @@ from nrpyelliptic_b200 import _lib
 from nrpyelliptic_b200.problem import CONFIGS, DeviceState, Problem
 
 pytestmark = pytest.mark.gpu
-TILE = 20  # both drivers on the same tile shape: identical L2 partial sums
+TILE = 15  # both drivers on the same tile shape: identical L2 partial sums
 
 
 @pytest.fixture(scope="module")

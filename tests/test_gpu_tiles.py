@@ -43,7 +43,7 @@ def tiles(lib):
 
 def test_tile_table_has_every_kind(lib):
     tl = tiles(lib)
-    assert {k for *_, k in tl} == {0, 2, 3, 4, 5}
+    assert {k for *_, k in tl} == {0, 2, 4, 5}
     assert lib.nrpyell_tile_info(len(tl), None, None, None) == -1
 
 
