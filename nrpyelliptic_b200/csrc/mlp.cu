@@ -5,7 +5,7 @@
 // guess.
 //
 // Every matrix product of the network -- forward Z = H W, backward
-// dH = dZ W^T and dW = H^T dZ -- is one kernel, k_gemm_tc: 128 x 64 output
+// dH = dZ W^T and dW = H^T dZ -- is one kernel, k_gemm_tc: 128 x 32 output
 // tiles, operands read with arbitrary strides (so the transposes are free),
 // rounded to BF16 into shared memory in the tensor cores' layout and
 // multiplied by tcgen05.mma issued from one thread, with the bias and tanh
@@ -28,19 +28,19 @@ namespace {
 // C[M x N] = alpha * A[M x K] B[K x N] (+ bias[N]) (then tanh), with
 // A(m,k) = A[m*sam + k*sak] and B(k,n) = B[k*sbk + n*sbn]; FP32 in and out.
 //
-// One CTA of 128 threads computes a 128 x 64 tile of C on the fifth-
+// One CTA of 128 threads computes a 128 x 32 tile of C on the fifth-
 // generation tensor cores: the operands are rounded to BF16 and written to
 // shared memory in the tensor cores' no-swizzle K-major layout (8 x 8
 // core matrices of 128 contiguous bytes), one thread issues
-// tcgen05.mma.cta_group::1.kind::f16 (M = 128, N = 64, K = 16) with the
+// tcgen05.mma.cta_group::1.kind::f16 (M = 128, N = 32, K = 16) with the
 // FP32 accumulator in tensor memory, tcgen05.commit signals an mbarrier when
 // the products of a 64-deep K chunk are done (the next chunk may then
 // overwrite shared memory), and each warp reads its 32 rows of the
 // accumulator back with tcgen05.ld for the epilogue (alpha, bias, tanh).
-constexpr int TC_M = 128, TC_N = 64, TC_KC = 64;      // CTA tile and K chunk
+constexpr int TC_M = 128, TC_N = 32, TC_KC = 64;      // CTA tile and K chunk
 constexpr int TC_B_OFF = 32 * 1024;                   // B tile at 32 KB (the 16 KB A tile at 0)
 constexpr int TC_SMEM = 64 * 1024;                    // dynamic shared memory per CTA
-constexpr int TC_TMEM_COLS = 128;                     // tensor-memory columns allocated (N = 64 used)
+constexpr int TC_TMEM_COLS = 128;                     // tensor-memory columns allocated (N = 32 used)
 constexpr int EPI_NONE = 0, EPI_BIAS = 1, EPI_BIAS_TANH = 2;
 constexpr long long kTcWaitLimit = 1ll << 22;         // bounded mbarrier wait (iterations)
 
@@ -117,9 +117,13 @@ __global__ void __launch_bounds__(128) k_gemm_tc(int M, int N, int K, const floa
   const int nchunks = (K + TC_KC - 1) / TC_KC;
   for (int c = 0; c < nchunks; c++) {
     const int k0 = c * TC_KC;
-    // A chunk: 128 rows x 32 k-pairs; B chunk: 64 rows (n) x 32 k-pairs
+    // A chunk: 128 rows x 32 k-pairs; B chunk: TC_N rows (n) x 32 k-pairs.
+    // Consecutive threads take consecutive k where the operand is contiguous
+    // along k, else consecutive rows, so the global loads coalesce.
+    const bool a_kfast = sak == 1, b_kfast = sbk == 1;
     for (int e = tid; e < TC_M * TC_KC / 2; e += 128) {
-      const int r = e / (TC_KC / 2), k = 2 * (e % (TC_KC / 2));
+      const int r = a_kfast ? e / (TC_KC / 2) : e % TC_M;
+      const int k = 2 * (a_kfast ? e % (TC_KC / 2) : e / TC_M);
       const int m = m0 + r, kk = k0 + k;
       float a0 = 0.f, a1 = 0.f;
       if (m < M) {
@@ -129,7 +133,8 @@ __global__ void __launch_bounds__(128) k_gemm_tc(int M, int N, int K, const floa
       *reinterpret_cast<uint32_t*>(As + tile_off<TC_M>(r, k)) = pack_bf16(a0, a1);
     }
     for (int e = tid; e < TC_N * TC_KC / 2; e += 128) {
-      const int r = e / (TC_KC / 2), k = 2 * (e % (TC_KC / 2));
+      const int r = b_kfast ? e / (TC_KC / 2) : e % TC_N;
+      const int k = 2 * (b_kfast ? e % (TC_KC / 2) : e / TC_N);
       const int n = n0 + r, kk = k0 + k;
       float b0 = 0.f, b1 = 0.f;
       if (n < N) {
@@ -165,11 +170,11 @@ __global__ void __launch_bounds__(128) k_gemm_tc(int M, int N, int K, const floa
   }
   asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory");
   if (!failed) {
-    // warp w reads accumulator rows 32w..32w+31 (tensor-memory lanes), 64 columns
+    // warp w reads accumulator rows 32w..32w+31 (tensor-memory lanes), TC_N columns
     const int m = m0 + 32 * warp + lane;
     const uint32_t taddr = tmem + ((uint32_t)(32 * warp) << 16);
 #pragma unroll
-    for (int half = 0; half < 2; half++) {
+    for (int half = 0; half < TC_N / 32; half++) {
       uint32_t v[32];
       asm volatile(
           "tcgen05.ld.sync.aligned.32x32b.x32.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15,%16,%17,%18,"

@@ -410,6 +410,15 @@ def main():
         ev.pop("u_zero")
     print()
     report(ev)
+    t = time.perf_counter()
+    cmp = compare_solvers(lib, guess, test_cfgs)
+    T["solver comparison"] = time.perf_counter() - t
+    print("\nheld-out solves, one form each (set-up outside the timings):")
+    for k in ("fp64_zero_guess", "fp64_learned", "mixed_learned", "batched_fp64_learned"):
+        v = cmp[k]
+        print("  %-22s %6.2f solves/s  RK4 steps median %6d  speed-up vs FP64 zero guess %.3f  fallbacks %s"
+              % (k, v["solves_per_s"], v["steps_median"], v.get("speedup_vs_fp64_zero_guess", 1.0),
+                 v.get("fallbacks", "-")))
     print("phase times: " + ", ".join("%s %.1f s" % kv for kv in T.items()))
     guess.free()
 
