@@ -331,7 +331,12 @@ int nrpyell_pod_guess(const float *mean, const float *basis, int K, long long nt
                       double *y_n);
 /* The same solve with host buffers: copies auxevol_host (3 gfs) and
  * y_n_host (2 gfs, the initial guess) to the device, relaxes, copies the
- * solution back into y_n_host. */
+ * solution back into y_n_host.  The library keeps one set of device
+ * gridfunction buffers between calls, reallocated when the point count
+ * changes.  Its device tables are cached by the addresses of the caller's
+ * bc_struct / rfm_struct arrays and xx plus the grid parameters: a caller
+ * that frees those arrays and reallocates them at the same addresses for a
+ * different grid must call nrpyell_release_tables() before the next call. */
 int nrpyell_relax_host(const paramstruct *params, REAL *xx[3], const bc_struct *bcstruct, const rfm_struct *rfmstruct,
                        const REAL *auxevol_host, REAL *y_n_host, const REAL dt, const REAL log10_tol, const int max_steps,
                        const REAL integration_radius, int *steps_taken, REAL *final_log10_l2);
