@@ -47,16 +47,22 @@ __global__ void __launch_bounds__(32 * BY) k_substep(SubDev<T> a) {
   __shared__ bool last;
   pdl_enter();
   if (*a.done) return;
-  if ((int)blockIdx.x < a.n_col_blocks) {
+  // 3-D grid (tiles0, tiles1, ncz + tiles2): the first ncz z-layers hold the
+  // column blocks (first in the launch), the rest the interior tiles, so the
+  // tile coordinates are the block indices themselves (no integer division)
+  const int ncz = a.ncz;
+  if ((int)blockIdx.z < ncz) {
+    const int cb = ((int)blockIdx.z * a.tiles1 + (int)blockIdx.y) * a.tiles0 + (int)blockIdx.x;
+    if (cb >= a.n_col_blocks) return;
     if constexpr (ROWS)
-      column_rows<T, STAGE, NT, CORR>(a, blockIdx.x, csm);
+      column_rows<T, STAGE, NT, CORR>(a, cb, csm);
     else
-      column_block<T, STAGE, NT>(a, blockIdx.x);
+      column_block<T, STAGE, NT>(a, cb);
     return;
   }
   const int tid = threadIdx.x;
-  const int b = blockIdx.x - a.n_col_blocks;
-  const int t0 = b % a.tiles0, t1 = (b / a.tiles0) % a.tiles1, t2 = b / (a.tiles0 * a.tiles1);
+  const int t0 = blockIdx.x, t1 = blockIdx.y, t2 = (int)blockIdx.z - ncz;
+  const int b = t0 + a.tiles0 * (t1 + a.tiles1 * t2);  // tile index (stop-test partials)
   const int i10 = t1 * BY + NGHOSTS;
   const int i0 = t0 * 32 + (tid & 31) + NGHOSTS;
   const int i1 = i10 + (tid >> 5);
@@ -411,7 +417,10 @@ static void launch_direct(const SubstepArgs& a) {
   constexpr int NT = 32 * BY;
   constexpr int CB = NT / kColThreadsPerColumn;
   f.n_col_blocks = NT >= 256 ? ((a.d.Nxx1 + kRows - 1) / kRows) * a.d.Nxx2 : (f.ncol + CB - 1) / CB;
-  NRPYELL_LAUNCH_PDL((k_substep<T, STAGE, RESID, BY, P, PF, CORR>), f.n_tiles + f.n_col_blocks, NT, 0, f);
+  const int plane = f.tiles0 * f.tiles1;
+  f.ncz = (f.n_col_blocks + plane - 1) / plane;
+  const dim3 grid(f.tiles0, f.tiles1, f.ncz + f.tiles2);
+  NRPYELL_LAUNCH_PDL((k_substep<T, STAGE, RESID, BY, P, PF, CORR>), grid, NT, 0, f);
 }
 
 template <typename T, int STAGE, bool RESID, int BY, int P>

@@ -24,6 +24,7 @@ struct SubDev {
   // planes (blocks first) and then chunks of msmall planes (blocks last)
   int mbig, msmall;
   int n_tiles, n_col_blocks, ncol;
+  int ncz;  // direct kernel: z-layers of its 3-D grid that hold the column blocks
   const T* __restrict__ S;     // stage input
   const T* y;                  // y_n (aliases out at stage 4)
   T* acc;
@@ -625,6 +626,7 @@ inline SubDev<T> make_dev(const SubstepArgs& a, int by, int p) {
   f.n_tiles = f.tiles0 * f.tiles1 * f.tiles2;
   f.mbig = f.tiles2;
   f.msmall = 0;
+  f.ncz = 0;
   f.ncol = d.Nxx1 * d.Nxx2;
   f.S = (const T*)a.S;
   f.y = (const T*)a.y;
