@@ -20,7 +20,7 @@ namespace nrpyell {
 namespace {
 
 constexpr int kBatchStepsPerGraph = 16;
-constexpr int kStateInts = 8;  // per grid: [0] n, [1] done, [2] converged, [3] stalled, [5] error
+constexpr int kStateInts = 8;  // per grid: [0] n, [1] done, [2] converged, [3] stalled
 
 struct BatchWork {
   int n = 0, hist_len = 0, partials_per = 0;

@@ -116,7 +116,6 @@ SubstepArgs substep_args(const Dims& d, RfmTables* rt, BcTables* bt, Scratch* s,
   a.stall_window = 0;
   a.stall_log_drop = 0.0;
   a.done = done;
-  a.err = state + 5;
   a.tile = tile;
   return a;
 }
@@ -282,7 +281,6 @@ RelaxResult relax_loop(const Dims& d, RfmTables* rt, BcTables* bt, L2Tables* lt,
     NRPYELL_CUDA(cudaEventCreateWithFlags(&ev[1], cudaEventDisableTiming));
   }
   NRPYELL_CUDA(cudaMemsetAsync(w->state, 0, sizeof(int) * 4, stream()));
-  NRPYELL_CUDA(cudaMemsetAsync(w->state + 5, 0, sizeof(int), stream()));
   const double stall_init[2] = {1e300, 0.0};
   NRPYELL_CUDA(cudaMemcpyAsync(w->stall, stall_init, sizeof(stall_init), cudaMemcpyHostToDevice, stream()));
   // Replay; poll the state of launch k-1 while launch k runs.
@@ -295,7 +293,7 @@ RelaxResult relax_loop(const Dims& d, RfmTables* rt, BcTables* bt, L2Tables* lt,
     NRPYELL_CUDA(cudaEventRecord(ev[slot], stream()));
     if (k > 0) {
       NRPYELL_CUDA(cudaEventSynchronize(ev[1 - slot]));
-      if (pinned[8 * (1 - slot) + 1] || pinned[8 * (1 - slot) + 5]) break;
+      if (pinned[8 * (1 - slot) + 1]) break;
     }
     if (!status_ok()) return res;
   }
@@ -303,12 +301,6 @@ RelaxResult relax_loop(const Dims& d, RfmTables* rt, BcTables* bt, L2Tables* lt,
   int st[6];
   NRPYELL_CUDA(cudaMemcpy(st, w->state, sizeof(st), cudaMemcpyDeviceToHost));
   if (!status_ok()) return res;
-  if (st[5]) {
-    char msg[128];
-    snprintf(msg, sizeof(msg), "fused substep: a bounded wait of a substep kernel gave up (code %d)", st[5]);
-    NRPYELL_FAIL(msg);
-    return res;
-  }
   res.steps = st[0];
   res.converged = st[2] != 0;
   res.stalled = st[3] != 0;

@@ -56,7 +56,6 @@ struct SubstepArgs {
   int stall_window;
   double stall_log_drop;
   const int* done;  // kernels return at entry when *done != 0
-  int* err;         // a kernel whose bounded wait gave up stores a nonzero code
   int tile;         // tile shape index (autotuned)
 };
 template <typename T>

@@ -42,7 +42,6 @@ struct SubDev {
   double* partials;
   unsigned int* ticket;
   int* state;  // [0] n, [1] done, [2] converged, [3] stalled
-  int* err;    // set to a nonzero code when a bounded wait gives up
   double* history;
   const int* done;
   double volume, log10_tol;
@@ -640,7 +639,6 @@ inline SubDev<T> make_dev(const SubstepArgs& a, int by, int p) {
   f.partials = a.s->partials;
   f.ticket = a.s->counter;
   f.state = a.state;
-  f.err = a.err;
   f.history = a.history;
   f.done = a.done;
   f.volume = a.lt ? a.lt->volume : 1.0;
