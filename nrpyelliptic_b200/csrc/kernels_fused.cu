@@ -35,8 +35,12 @@ namespace nrpyell {
 // ------------------------------------------------------- direct interior
 // CORR: the correction form of the mixed-precision driver
 // (point_rhs_correction; 8-warp shapes without PF only).
-template <typename T, int STAGE, bool RESID, int BY, int P, bool PF, bool CORR = false>
-__global__ void __launch_bounds__(32 * BY) k_substep(SubDev<T> a) {
+// At least MINB resident blocks per SM, which caps the registers.  The
+// default caps the one-plane shapes at 1024 threads per SM (64 registers,
+// which they fit without spilling) and leaves the others to the compiler.
+template <typename T, int STAGE, bool RESID, int BY, int P, bool PF, bool CORR = false,
+          int MINB = (P == 1 && !PF) ? 32 / BY : 1>
+__global__ void __launch_bounds__(32 * BY, MINB) k_substep(SubDev<T> a) {
   constexpr int NT = 32 * BY;
   static_assert(!CORR || (NT >= 256 && !PF), "the correction form runs on 8-warp shapes without PF");
   __shared__ double sh[NT / 32 > 8 ? NT / 32 : 8];
@@ -403,7 +407,8 @@ int substep_interior_blocks(const Dims& d, int tile) {
 template <typename T, int STAGE, bool RESID, int BY, int P>
 static void launch_planes(const SubstepArgs& a);
 
-template <typename T, int STAGE, bool RESID, int BY, int P, bool PF, bool CORR = false>
+template <typename T, int STAGE, bool RESID, int BY, int P, bool PF, bool CORR = false,
+          int MINB = (P == 1 && !PF) ? 32 / BY : 1>
 static void launch_direct(const SubstepArgs& a) {
   if (!march_fits(a.d)) {  // 64-bit offsets: the planes kernel
     if (CORR) {
@@ -420,7 +425,7 @@ static void launch_direct(const SubstepArgs& a) {
   const int plane = f.tiles0 * f.tiles1;
   f.ncz = (f.n_col_blocks + plane - 1) / plane;
   const dim3 grid(f.tiles0, f.tiles1, f.ncz + f.tiles2);
-  NRPYELL_LAUNCH_PDL((k_substep<T, STAGE, RESID, BY, P, PF, CORR>), grid, NT, 0, f);
+  NRPYELL_LAUNCH_PDL((k_substep<T, STAGE, RESID, BY, P, PF, CORR, MINB>), grid, NT, 0, f);
 }
 
 template <typename T, int STAGE, bool RESID, int BY, int P>
