@@ -37,9 +37,11 @@ namespace nrpyell {
 // (point_rhs_correction; 8-warp shapes without PF only).
 // At least MINB resident blocks per SM, which caps the registers.  The
 // default caps the one-plane shapes at 1024 threads per SM (64 registers,
-// which they fit without spilling) and leaves the others to the compiler.
+// which they fit without spilling) and the two-plane 8-warp shape at 3
+// blocks per SM (78 registers, no spills; 47.0 -> 40.8 us per RK4 step at
+// 128x128x16), and leaves the prefetching shapes to the compiler.
 template <typename T, int STAGE, bool RESID, int BY, int P, bool PF, bool CORR = false,
-          int MINB = (P == 1 && !PF) ? 32 / BY : 1>
+          int MINB = PF ? 1 : (P == 1 ? 32 / BY : (BY == 8 && P == 2 ? 3 : 1))>
 __global__ void __launch_bounds__(32 * BY, MINB) k_substep(SubDev<T> a) {
   constexpr int NT = 32 * BY;
   static_assert(!CORR || (NT >= 256 && !PF), "the correction form runs on 8-warp shapes without PF");
@@ -408,7 +410,7 @@ template <typename T, int STAGE, bool RESID, int BY, int P>
 static void launch_planes(const SubstepArgs& a);
 
 template <typename T, int STAGE, bool RESID, int BY, int P, bool PF, bool CORR = false,
-          int MINB = (P == 1 && !PF) ? 32 / BY : 1>
+          int MINB = PF ? 1 : (P == 1 ? 32 / BY : (BY == 8 && P == 2 ? 3 : 1))>
 static void launch_direct(const SubstepArgs& a) {
   if (!march_fits(a.d)) {  // 64-bit offsets: the planes kernel
     if (CORR) {
