@@ -85,3 +85,21 @@ def test_auxevol_on_the_gpu_matches_the_host_set_up(lib):
             assert np.max(np.abs(aux[g] - ref[g])) <= 1e-13 * np.max(np.abs(ref[g])), (cfg.name, g)
         assert dev.params.uu_wavespeed_at_OB == pytest.approx(host.params.uu_wavespeed_at_OB, rel=1e-14)
         ds.free()
+
+
+def test_batch_on_sweep_grids_matches_single_runs(lib):
+    """Three draws of the sweep distribution on its own grids (96x96x12 and
+    128x128x16, tables and auxevol built on the GPU; the batch's shape
+    autotuned) against single-grid relaxations: the same steps and the same
+    bits (every tile shape gives identical steps, test_gpu_tiles)."""
+    cfgs = [c for c in sample_sweep(64) if c.Nxx in ((96, 96, 12), (128, 128, 16))][:3]
+    assert len(cfgs) == 3
+    probs = [Problem(c, lib=lib, host_aux=False, device_tables=True) for c in cfgs]
+    rc, steps, finals, states = relax_batch(probs, tol=-10.0, max_steps=20000, lib=lib)
+    assert rc == 0 and np.all(finals <= -10.0)
+    for i, p in enumerate(probs):
+        rc1, s1, f1, y1 = _alone(lib, p, 20000)
+        assert rc1 == 0 and steps[i] == s1 and finals[i] == f1, (cfgs[i].name, steps[i], s1)
+        np.testing.assert_array_equal(states[i].download("y_n"), y1, err_msg=cfgs[i].name)
+    for s in states:
+        s.free()
