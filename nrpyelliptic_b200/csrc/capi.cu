@@ -578,7 +578,7 @@ int nrpyell_relax(griddata_struct* g, const REAL dt, const REAL log10_tol, const
   RelaxParams rp = relax_params(&g->params, dt);
   rp.log10_tol = log10_tol;
   rp.max_steps = max_steps;
-  const int tile = tuned_tile<double>(su.d, su.rt, su.bt, su.w, su.s, b, rp);
+  const int tile = tuned_tile<double>(su.d, su.rt, su.bt, su.w, su.s, b, rp, su.lt);
   const RelaxResult r = relax_loop<double>(su.d, su.rt, su.bt, su.lt, su.w, su.s, tile, b, rp);
   // ghost zones of the solution, as the reference's all-points update leaves them
   launch_ghost_fill<double>(su.d, su.bt, g->gridfuncs.y_n_gfs);
@@ -607,7 +607,7 @@ int nrpyell_relax_et(griddata_struct* g, const REAL dt, const REAL log_target_re
   rp.log10_tol = log_target_residual;
   rp.max_steps = max_iterations + 1;
   rp.check_every = check_every;
-  const int tile = tuned_tile<double>(su.d, su.rt, su.bt, su.w, su.s, b, rp);
+  const int tile = tuned_tile<double>(su.d, su.rt, su.bt, su.w, su.s, b, rp, su.lt);
   const RelaxResult r = relax_loop<double>(su.d, su.rt, su.bt, su.lt, su.w, su.s, tile, b, rp);
   launch_ghost_fill<double>(su.d, su.bt, g->gridfuncs.y_n_gfs);
   NRPYELL_CUDA(cudaStreamSynchronize(stream()));
@@ -703,7 +703,7 @@ int nrpyell_relax_mixed(griddata_struct* g, const REAL dt, const REAL log10_tol,
     // log10_switch, and is folded into U.
     NRPYELL_CUDA(cudaMemsetAsync(b32.y, 0, sizeof(float) * n2, stream()));
     rp.max_steps = std::min(cycle_len, max_steps - n);
-    if (tile32 < 0) tile32 = tuned_tile<float>(d, su.rt, su.bt, w, su.s, b32, rp);
+    if (tile32 < 0) tile32 = tuned_tile<float>(d, su.rt, su.bt, w, su.s, b32, rp, su.lt);
     const RelaxResult r = relax_loop<float>(d, su.rt, su.bt, su.lt, w, su.s, tile32, b32, rp);
     if (!status_ok()) return -1;
     launch_correction_fold(U, (const float*)b32.y, n2);
@@ -722,7 +722,7 @@ int nrpyell_relax_mixed(griddata_struct* g, const REAL dt, const REAL log10_tol,
     rp64.log10_tol = log10_tol;
     rp64.max_steps = max_steps - n;
     rp64.history_offset = n;
-    const int tile64 = tuned_tile<double>(d, su.rt, su.bt, w, su.s, b64, rp64);
+    const int tile64 = tuned_tile<double>(d, su.rt, su.bt, w, su.s, b64, rp64, su.lt);
     const RelaxResult r64 = relax_loop<double>(d, su.rt, su.bt, su.lt, w, su.s, tile64, b64, rp64);
     n64 = r64.steps;
     converged = r64.converged;

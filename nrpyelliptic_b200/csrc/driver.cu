@@ -120,40 +120,46 @@ SubstepArgs substep_args(const Dims& d, RfmTables* rt, BcTables* bt, Scratch* s,
   return a;
 }
 
-// Tile-shape autotuner: times the stage-2 fused substep (the most common
-// kind) for every tile shape on the caller's own buffers and keeps the
-// fastest, once per grid size and precision.  The timing launches write only
-// the running-total and k_even buffers, which every RK4 step overwrites
-// before reading.  Each shape gets a warm-up launch and the best of three
-// 10-launch timings.
+// Tile-shape autotuner: times every tile shape on the caller's own buffers
+// and keeps the fastest, once per grid size and precision (and form).  Each
+// shape is timed on whole RK4 steps as the relaxation runs them -- stage 1
+// storing its residual partials when an L2 table is given (the per-tile
+// reduction depends on the shape), then stages 2, 3 and 4 -- one warm-up
+// step and the best of three 4-step timings.  Stage 4 writes y_n, so y_n is
+// saved before the timings and restored after them.
 template <typename T>
 int tuned_tile(const Dims& d, RfmTables* rt, BcTables* bt, FusedWork* w, Scratch* sc, const StateBuffers& b,
-               const RelaxParams& rp) {
+               const RelaxParams& rp, const L2Tables* lt) {
   // the correction form runs on the marching and 8-warp direct shapes
   const bool corr = b.R0 != nullptr;
   const int which = sizeof(T) == 8 ? 0 : (corr ? 2 : 1);
   if (g_forced_tile >= 0 && !(corr && !substep_supports_correction(g_forced_tile))) return g_forced_tile;
   if (w->tile[which] >= 0) return w->tile[which];
+  const size_t ybytes = sizeof(T) * 2 * (size_t)d.Ntot;
+  void* ysave = nullptr;
+  NRPYELL_CUDA(dev_alloc(&ysave, ybytes));
+  if (!status_ok()) return 0;
+  NRPYELL_CUDA(cudaMemcpyAsync(ysave, b.y, ybytes, cudaMemcpyDeviceToDevice, stream()));
   cudaEvent_t e0, e1;
   NRPYELL_CUDA(cudaEventCreate(&e0));
   NRPYELL_CUDA(cudaEventCreate(&e1));
   int best = -1;
   float best_ms = 1e30f;
-  // Each shape is timed on stages 1-3 back to back, as a relaxation runs
-  // them (a shape can be fast at one stage and slow at the next); stage 4
-  // would write y_n, the caller's state, so it is left out -- stages 1-3
-  // write only the running total and the stage buffers.
   for (int t = 0; t < substep_num_tiles(); t++) {
     if (corr && (!substep_supports_correction(t) || !march_fits(d))) continue;
-    SubstepArgs a[3];
-    for (int st = 1; st <= 3; st++) a[st - 1] = substep_args(d, rt, bt, sc, b, rp, st, w->zero_flag, w->state, t);
+    SubstepArgs a[4];
+    for (int st = 1; st <= 4; st++) a[st - 1] = substep_args(d, rt, bt, sc, b, rp, st, w->zero_flag, w->state, t);
+    if (lt) {
+      a[0].lt = lt;
+      a[0].defer_l2 = 1;  // partials only, as in relax_loop (no stop test here)
+    }
     prepare_substep<T>(t);
-    for (int st = 1; st <= 3; st++) launch_substep<T>(st, a[st - 1]);
+    for (int st = 1; st <= 4; st++) launch_substep<T>(st, a[st - 1]);
     float tmin = 1e30f;
     for (int rep = 0; rep < 3; rep++) {
       NRPYELL_CUDA(cudaEventRecord(e0, stream()));
       for (int i = 0; i < 4; i++)
-        for (int st = 1; st <= 3; st++) launch_substep<T>(st, a[st - 1]);
+        for (int st = 1; st <= 4; st++) launch_substep<T>(st, a[st - 1]);
       NRPYELL_CUDA(cudaEventRecord(e1, stream()));
       NRPYELL_CUDA(cudaEventSynchronize(e1));
       float ms = 0.0f;
@@ -165,6 +171,9 @@ int tuned_tile(const Dims& d, RfmTables* rt, BcTables* bt, FusedWork* w, Scratch
       best = t;
     }
   }
+  NRPYELL_CUDA(cudaMemcpyAsync(b.y, ysave, ybytes, cudaMemcpyDeviceToDevice, stream()));
+  NRPYELL_CUDA(cudaStreamSynchronize(stream()));
+  NRPYELL_CUDA(cudaFree(ysave));
   NRPYELL_CUDA(cudaEventDestroy(e0));
   NRPYELL_CUDA(cudaEventDestroy(e1));
   if (best < 0) {
@@ -175,9 +184,9 @@ int tuned_tile(const Dims& d, RfmTables* rt, BcTables* bt, FusedWork* w, Scratch
   return best;
 }
 template int tuned_tile<double>(const Dims&, RfmTables*, BcTables*, FusedWork*, Scratch*, const StateBuffers&,
-                                const RelaxParams&);
+                                const RelaxParams&, const L2Tables*);
 template int tuned_tile<float>(const Dims&, RfmTables*, BcTables*, FusedWork*, Scratch*, const StateBuffers&,
-                               const RelaxParams&);
+                               const RelaxParams&, const L2Tables*);
 
 // ------------------------------------------------------------ relax loop
 // A CUDA graph of kStepsPerGraph RK4 steps is replayed until the device-side

@@ -67,9 +67,12 @@ int max_interior_blocks(const Dims& d);
 StateBuffers buffers_of(const MoL_gridfunctions_struct* gf);
 SubstepArgs substep_args(const Dims& d, RfmTables* rt, BcTables* bt, Scratch* s, const StateBuffers& b,
                          const RelaxParams& rp, int stage, const int* done, int* state, int tile);
+// Autotuned tile shape of this grid size, precision and form; lt (nullable):
+// time stage 1 with the relaxation's residual partials.  Never call while a
+// stream is being captured (it allocates a copy of y_n).
 template <typename T>
 int tuned_tile(const Dims& d, RfmTables* rt, BcTables* bt, FusedWork* w, Scratch* sc, const StateBuffers& b,
-               const RelaxParams& rp);
+               const RelaxParams& rp, const L2Tables* lt = nullptr);
 template <typename T>
 RelaxResult relax_loop(const Dims& d, RfmTables* rt, BcTables* bt, L2Tables* lt, FusedWork* w, Scratch* s, int tile,
                        const StateBuffers& b, const RelaxParams& rp);
