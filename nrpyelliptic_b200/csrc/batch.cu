@@ -20,12 +20,11 @@ namespace nrpyell {
 namespace {
 
 constexpr int kBatchStepsPerGraph = 16;
-constexpr int kStateInts = 8;  // per grid: [0] n, [1] done, [2] converged, [3] stalled
+constexpr int kStateInts = 8;  // per grid: [0] n, [1] done, [2] converged
 
 struct BatchWork {
   int n = 0, hist_len = 0, partials_per = 0;
   int* state = nullptr;     // n x kStateInts
-  double* stall = nullptr;  // n x 2
   double* history = nullptr;
   double* partials = nullptr;
   unsigned int* tickets = nullptr;
@@ -36,7 +35,6 @@ BatchWork g_batch;
 
 void free_batch() {
   cudaFree(g_batch.state);
-  cudaFree(g_batch.stall);
   cudaFree(g_batch.history);
   cudaFree(g_batch.partials);
   cudaFree(g_batch.tickets);
@@ -53,7 +51,6 @@ bool ensure_batch(int n, int hist_len, int partials_per) {
   g_batch.hist_len = hist_len;
   g_batch.partials_per = partials_per;
   NRPYELL_CUDA(dev_alloc(&g_batch.state, sizeof(int) * kStateInts * n));
-  NRPYELL_CUDA(dev_alloc(&g_batch.stall, sizeof(double) * 2 * n));
   NRPYELL_CUDA(dev_alloc(&g_batch.history, sizeof(double) * (size_t)hist_len * n));
   NRPYELL_CUDA(dev_alloc(&g_batch.partials, sizeof(double) * (size_t)partials_per * n));
   NRPYELL_CUDA(dev_alloc(&g_batch.tickets, sizeof(unsigned int) * n));
@@ -96,8 +93,6 @@ bool build_devs(const std::vector<Grid>& grids, int tile, std::vector<SubDev<dou
         a.history = g_batch.history + (size_t)c * g_batch.hist_len;
         a.log10_tol = g.rp.log10_tol;
         a.max_steps = g.rp.max_steps;
-        a.stall = g_batch.stall + 2 * c;
-        a.stall_window = 0;
       }
       if (!batch_launch_dev<double>(a, &(*devs)[k * n + c])) return false;
     }
@@ -216,14 +211,7 @@ extern "C" int nrpyell_relax_batch(const int n, griddata_struct* grids, const RE
   }
   if (tile < 0 || !build_devs(gs, tile, &devs, &offs, &blocks) || !upload_devs(devs, offs)) return -1;
   NRPYELL_CUDA(cudaMemsetAsync(g_batch.state, 0, sizeof(int) * kStateInts * n, stream()));
-  std::vector<double> stall_init(2 * n);
-  for (int c = 0; c < n; c++) {
-    stall_init[2 * c] = 1e300;
-    stall_init[2 * c + 1] = 0.0;
-  }
-  NRPYELL_CUDA(cudaMemcpyAsync(g_batch.stall, stall_init.data(), sizeof(double) * 2 * n, cudaMemcpyHostToDevice,
-                               stream()));
-  NRPYELL_CUDA(cudaStreamSynchronize(stream()));  // stall_init leaves scope below only after this
+  NRPYELL_CUDA(cudaStreamSynchronize(stream()));
   if (!status_ok()) return -1;
 
   // capture sixteen RK4 steps of the whole batch

@@ -36,7 +36,6 @@ FusedWork* get_work(const Dims& d, int history_len) {
   NRPYELL_CUDA(dev_alloc(&w->state, sizeof(int) * 8 + sizeof(double) * 4));
   NRPYELL_CUDA(cudaMemset(w->state, 0, sizeof(int) * 8 + sizeof(double) * 4));
   w->zero_flag = w->state + 4;
-  w->stall = (double*)(w->state + 8);
   w->history_len = history_len > 16 ? history_len : 16;
   NRPYELL_CUDA(dev_alloc(&w->history, sizeof(double) * w->history_len));
   g_work.push_back(w);
@@ -112,9 +111,6 @@ SubstepArgs substep_args(const Dims& d, RfmTables* rt, BcTables* bt, Scratch* s,
   a.max_steps = 0;
   a.check_every = 0;
   a.defer_l2 = 0;
-  a.stall = nullptr;
-  a.stall_window = 0;
-  a.stall_log_drop = 0.0;
   a.done = done;
   a.tile = tile;
   return a;
@@ -219,7 +215,7 @@ void release_graphs() {
 template <typename T>
 RelaxResult relax_loop(const Dims& d, RfmTables* rt, BcTables* bt, L2Tables* lt, FusedWork* w, Scratch* s, int tile,
                        const StateBuffers& b, const RelaxParams& rp) {
-  RelaxResult res = {0, false, false, NAN};
+  RelaxResult res = {0, false, NAN};
   const int fp32 = sizeof(T) == 4;
   RelaxGraph* rg = nullptr;
   for (size_t i = 0; i < g_graphs.size(); i++) {
@@ -250,9 +246,6 @@ RelaxResult relax_loop(const Dims& d, RfmTables* rt, BcTables* bt, L2Tables* lt,
       a1.log10_tol = rp.log10_tol;
       a1.max_steps = rp.max_steps;
       a1.check_every = rp.check_every;
-      a1.stall = w->stall;
-      a1.stall_window = rp.stall_window;
-      a1.stall_log_drop = rp.stall_log_drop;
       a1.defer_l2 = 1;
       launch_substep<T>(1, a1);
       launch_finalize_forked<T>(a1);  // the norm and stop test beside stage 2
@@ -290,8 +283,6 @@ RelaxResult relax_loop(const Dims& d, RfmTables* rt, BcTables* bt, L2Tables* lt,
     NRPYELL_CUDA(cudaEventCreateWithFlags(&ev[1], cudaEventDisableTiming));
   }
   NRPYELL_CUDA(cudaMemsetAsync(w->state, 0, sizeof(int) * 4, stream()));
-  const double stall_init[2] = {1e300, 0.0};
-  NRPYELL_CUDA(cudaMemcpyAsync(w->stall, stall_init, sizeof(stall_init), cudaMemcpyHostToDevice, stream()));
   // Replay; poll the state of launch k-1 while launch k runs.
   const long long max_launches = (long long)rp.max_steps / kStepsPerGraph + 2;
   for (long long k = 0; k < max_launches; k++) {
@@ -312,7 +303,6 @@ RelaxResult relax_loop(const Dims& d, RfmTables* rt, BcTables* bt, L2Tables* lt,
   if (!status_ok()) return res;
   res.steps = st[0];
   res.converged = st[2] != 0;
-  res.stalled = st[3] != 0;
   NRPYELL_CUDA(cudaMemcpy(&res.last_log10_l2, (rp.history_buf ? rp.history_buf : w->history) + rp.history_offset + st[0],
                           sizeof(double), cudaMemcpyDeviceToHost));
   return res;

@@ -11,9 +11,8 @@ namespace nrpyell {
 // Per-grid driver state on the device.
 struct FusedWork {
   Dims d;
-  int* state;      // [0] n, [1] done, [2] converged, [3] stalled
+  int* state;      // [0] n, [1] done, [2] converged
   int* zero_flag;  // always 0 (single steps run unconditionally)
-  double* stall;   // [0] log10 L2 at the start of the stall window, [1] its step
   double* history;
   int history_len;
   int tile[3];     // autotuned tile for FP64 / FP32 / FP32 correction form, -1 = not tuned yet
@@ -39,15 +38,13 @@ struct RelaxParams {
   double log10_tol;
   int max_steps;
   int check_every;  // 0: stop test on every residual (main.c); > 0: ET thorn semantics
-  int stall_window;       // 0: no stall test
-  double stall_log_drop;  // stalled when log10 L2 fell by less than this over the window (negative)
   int history_offset;     // history index of step 0 of this run
   double* history_buf;    // where the history goes (nullptr: the work's own)
 };
 
 struct RelaxResult {
   int steps;  // index n of the last evaluated residual
-  bool converged, stalled;
+  bool converged;
   double last_log10_l2;
 };
 

@@ -49,12 +49,6 @@ struct SubstepArgs {
   // 1: the stage-1 blocks only store their per-tile partials and the norm
   // and stop test are left to launch_finalize_forked (relaxation driver).
   int defer_l2;
-  // Optional stall test: stop (state[3] = 1) once the best log10 L2 so far
-  // has not dropped by at least -stall_log_drop for stall_window steps;
-  // stall[0..1] = best log10 L2 and the step it was reached.
-  double* stall;
-  int stall_window;
-  double stall_log_drop;
   const int* done;  // kernels return at entry when *done != 0
   int tile;         // tile shape index (autotuned)
 };

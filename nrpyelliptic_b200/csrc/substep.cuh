@@ -41,16 +41,13 @@ struct SubDev {
   const double* __restrict__ w;  // L2 weights (stage-1 residual)
   double* partials;
   unsigned int* ticket;
-  int* state;  // [0] n, [1] done, [2] converged, [3] stalled
+  int* state;  // [0] n, [1] done, [2] converged
   double* history;
   const int* done;
   double volume, log10_tol;
   int max_steps;
   int check_every;  // > 0: Einstein Toolkit thorn semantics (see finalize_l2)
   int defer_l2;     // stage 1: store the per-tile partials only (k_finalize_l2 reduces them)
-  double* stall;
-  int stall_window;
-  double stall_log_drop;
   T dt, eta;
   T cOB[2];
   double invdx0, invdx1;
@@ -239,20 +236,6 @@ __device__ void finalize_l2(const SubDev<T>& a, double* sh) {
     const double l2 = log10(1e-16 + sqrt(tot / a.volume));
     const int n = a.state[0];
     if (a.history) a.history[n] = l2;
-    // Stall test on the best residual so far: the relaxation residual
-    // oscillates (and grows for a while after a cold start), so only a lack
-    // of progress of the running minimum over a whole window counts, and only
-    // once that minimum is within two decades of the tolerance of this phase
-    // -- a precision floor shows up there.
-    bool stalled = false;
-    if (a.stall_window > 0) {
-      if (n == 0 || l2 < a.stall[0] + a.stall_log_drop) {
-        a.stall[0] = l2;
-        a.stall[1] = (double)n;
-      } else if (n - (int)a.stall[1] >= a.stall_window && a.stall[0] <= a.log10_tol + 2.0) {
-        stalled = true;
-      }
-    }
     // main.c semantics: the stop test on every residual, log10 L2 <= tol.
     // The ET thorn's (NRPyEllipticET_..._Hyperbolic_Relaxation.c:185-217):
     // its loop index counts steps already taken minus one, it tests after
@@ -262,9 +245,6 @@ __device__ void finalize_l2(const SubDev<T>& a, double* sh) {
     const bool met = test && (a.check_every > 0 ? l2 < a.log10_tol : l2 <= a.log10_tol);
     if (met) {
       a.state[2] = 1;
-      a.state[1] = 1;
-    } else if (stalled) {
-      a.state[3] = 1;
       a.state[1] = 1;
     } else if (n >= a.max_steps) {
       a.state[1] = 1;
@@ -646,9 +626,6 @@ inline SubDev<T> make_dev(const SubstepArgs& a, int by, int p) {
   f.max_steps = a.max_steps;
   f.check_every = a.check_every;
   f.defer_l2 = a.defer_l2;
-  f.stall = a.stall;
-  f.stall_window = a.stall_window;
-  f.stall_log_drop = a.stall_log_drop;
   f.dt = (T)a.dt;
   f.eta = (T)a.eta;
   f.cOB[0] = (T)a.cOB[0];

@@ -35,7 +35,7 @@ def test_profiled_traffic_reads_each_kernel_and_grid():
 
 def test_every_tile_kind_names_a_kernel():
     bench = _bench()
-    # kinds of nrpyell_tile_info: 0 direct, 2 direct with prefetch, 3 TMA
-    # pipeline, 4 shared-memory planes, 5 marching
+    # kinds of nrpyell_tile_info: 0 direct, 2 direct with prefetch, 4
+    # shared-memory planes, 5 marching
     assert set(bench.KERNELS) == {0, 2, 4, 5}
     assert bench.KERNELS[5] == "k_substep_march" and bench.KERNELS[4] == "k_substep_planes"

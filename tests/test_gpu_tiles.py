@@ -1,5 +1,5 @@
-"""Every tile shape of the fused substep kernel (direct, prefetching, TMA
-pipeline, shared-memory planes, marching along i2) against the reference's
+"""Every tile shape of the fused substep kernel (direct, prefetching,
+shared-memory planes, marching along i2) against the reference's
 golden steps and against each other.
 
 The shapes differ only in how points are assigned to threads and how the
