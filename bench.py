@@ -359,7 +359,7 @@ def learned_leg(lib, args):
     """The learned initial guess on the 128x128x16 sweep distribution with a
     reduced training set (args.learned_train batched training solves, 64 POD
     modes, 300 epochs): the plain FP64 form against the learned guess alone,
-    with the mixed-precision driver and with the batched driver, on
+    with the mixed-precision driver, with the batched driver and with both, on
     args.learned_test held-out draws (nrpyelliptic_b200.learned.compare_solvers)."""
     from nrpyelliptic_b200 import learned
     t0 = time.perf_counter()

@@ -306,6 +306,20 @@ int nrpyell_initial_lapse(const paramstruct *params, int npts, const REAL *xyz, 
  * error. */
 int nrpyell_relax_batch(int n, griddata_struct *grids, const REAL *dt, REAL log10_tol, int max_steps,
                         REAL integration_radius, int *steps_taken, REAL *final_log10_l2);
+/* nrpyell_relax_mixed on a batch: each configuration follows the
+ * single-grid schedule (FP64 evaluation and stop test of its base state, an
+ * FP32 correction stretch of up to fold_every steps or to log10_switch, the
+ * fold; FP64 steps from the switch on), and the stretches of all
+ * configurations still in the FP32 phase, then their FP64 phases, run as
+ * batches (marching shapes for the FP32 stretches).  With the same tile
+ * shapes each configuration's result is bitwise that of nrpyell_relax_mixed.
+ * steps_fp32[c], steps_fp64[c], final_log10_l2[c] as there (each array may
+ * be NULL); the FP32 buffers (15 Ntot floats per configuration) stay
+ * allocated for later calls until nrpyell_release_tables.  Returns the number
+ * of configurations that did not converge, < 0 on error. */
+int nrpyell_relax_batch_mixed(int n, griddata_struct *grids, const REAL *dt, REAL log10_tol, REAL log10_switch,
+                              int fold_every, int max_steps, REAL integration_radius, int *steps_fp32,
+                              int *steps_fp64, REAL *final_log10_l2);
 /* Learned initial guess (BF16 tensor-core MLP, FP32 master weights, Adam).
  * The network maps n_in inputs through `depth` tanh layers of `width` to
  * n_out linear outputs.  All arrays are device pointers unless named host.

@@ -93,6 +93,8 @@ EXPORTS = {
                                                PREAL, PREAL]),
     "nrpyell_relax_batch": (C.c_int, [C.c_int, P(abi.griddata_struct), PREAL, C.c_double, C.c_int, C.c_double,
                                       P(C.c_int), PREAL]),
+    "nrpyell_relax_batch_mixed": (C.c_int, [C.c_int, P(abi.griddata_struct), PREAL, C.c_double, C.c_double, C.c_int,
+                                            C.c_int, C.c_double, P(C.c_int), P(C.c_int), PREAL]),
     "nrpyell_mlp_create": (C.c_void_p, [C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, C.c_uint]),
     "nrpyell_mlp_destroy": (None, [C.c_void_p]),
     "nrpyell_mlp_num_params": (C.c_longlong, [C.c_void_p]),

@@ -36,6 +36,23 @@ def relax_batch(problems, states=None, tol=-10.0, max_steps=100000, lib=None):
     return rc, np.array(steps[:], dtype=np.int64), finals, states
 
 
+def relax_batch_mixed(problems, states=None, tol=-10.0, switch=-10.0, fold_every=256, max_steps=100000, lib=None):
+    """The FP32 correction form (nrpyell_relax_batch_mixed) on `problems`
+    together, from the zero guess or from `states`.  Returns
+    (n_not_converged, steps_fp32, steps_fp64, final_log10_l2, states)."""
+    lib = lib or _lib.load()
+    n = len(problems)
+    states = states or [DeviceState(p, lib=lib) for p in problems]
+    grids = (abi.griddata_struct * n)(*[s.g for s in states])
+    dts = np.array([p.dt for p in problems], dtype=np.float64)
+    s32, s64 = (C.c_int * n)(), (C.c_int * n)()
+    finals = np.zeros(n)
+    rc = lib.nrpyell_relax_batch_mixed(n, grids, dts.ctypes.data_as(abi.PREAL), tol, switch, fold_every, max_steps,
+                                       float(problems[0].cfg.R_L2), s32, s64, finals.ctypes.data_as(abi.PREAL))
+    _lib.check(lib)
+    return (rc, np.array(s32[:], dtype=np.int64), np.array(s64[:], dtype=np.int64), finals, states)
+
+
 def solve_batch(cfgs, lib=None, tol=-10.0, max_steps=100000, device_tables=True):
     """Set up cfgs (tables and auxevol on the GPU) and relax them together in
     one batch; per configuration a dict with its RK4 steps, final log10 L2

@@ -595,6 +595,7 @@ bool batch_launch_dev(const SubstepArgs& a, SubDev<T>* out) {
   return true;
 }
 template bool batch_launch_dev<double>(const SubstepArgs&, SubDev<double>*);
+template bool batch_launch_dev<float>(const SubstepArgs&, SubDev<float>*);
 
 template <typename T, int STAGE, bool RESID>
 static void launch_batch_stage(int tile, const SubDev<T>* devs, const int* offs, int n, int blocks) {
@@ -616,25 +617,32 @@ static void launch_batch_stage(int tile, const SubDev<T>* devs, const int* offs,
 }
 
 template <typename T>
-void launch_substep_batch(int stage, bool resid, int tile, const SubDev<T>* devs, const int* offs, int n,
-                          int blocks) {
+void launch_substep_batch(int stage, bool resid, int tile, const SubDev<T>* devs, const int* offs, int n, int blocks,
+                          bool corr) {
   if (kTiles[tile].kind == 5) {  // batch_launch_dev checked march_fits for every grid
-    launch_march_batch<T>(stage, resid, kTiles[tile].v, devs, offs, n, blocks);
+    launch_march_batch<T>(stage, resid, kTiles[tile].v, devs, offs, n, blocks, corr);
     return;
   }
-  switch (stage) {
-    case 1:
-      if (resid)
-        launch_batch_stage<T, 1, true>(tile, devs, offs, n, blocks);
-      else
-        launch_batch_stage<T, 1, false>(tile, devs, offs, n, blocks);
-      break;
-    case 2: launch_batch_stage<T, 2, false>(tile, devs, offs, n, blocks); break;
-    case 3: launch_batch_stage<T, 3, false>(tile, devs, offs, n, blocks); break;
-    default: launch_batch_stage<T, 4, false>(tile, devs, offs, n, blocks); break;
+  if (corr || sizeof(T) != 8) {
+    NRPYELL_FAIL("batched substep: FP32 and the correction form run on the marching shapes only");
+    return;
+  }
+  if constexpr (sizeof(T) == 8) {
+    switch (stage) {
+      case 1:
+        if (resid)
+          launch_batch_stage<T, 1, true>(tile, devs, offs, n, blocks);
+        else
+          launch_batch_stage<T, 1, false>(tile, devs, offs, n, blocks);
+        break;
+      case 2: launch_batch_stage<T, 2, false>(tile, devs, offs, n, blocks); break;
+      case 3: launch_batch_stage<T, 3, false>(tile, devs, offs, n, blocks); break;
+      default: launch_batch_stage<T, 4, false>(tile, devs, offs, n, blocks); break;
+    }
   }
 }
-template void launch_substep_batch<double>(int, bool, int, const SubDev<double>*, const int*, int, int);
+template void launch_substep_batch<double>(int, bool, int, const SubDev<double>*, const int*, int, int, bool);
+template void launch_substep_batch<float>(int, bool, int, const SubDev<float>*, const int*, int, int, bool);
 
 template <typename T>
 void launch_ghost_fill(const Dims& d, const BcTables* bt, void* gfs) {

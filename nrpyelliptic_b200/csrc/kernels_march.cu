@@ -280,7 +280,7 @@ __global__ void __launch_bounds__(32 * BY, MINB) k_substep_march(SubDev<T> a) {
 // One substep of many grids in one launch: the blocks of grid c are
 // offs[c] .. offs[c+1]-1 (column blocks first, then interior tiles), each
 // grid with its own launch arguments, stop test and done flag.
-template <typename T, int STAGE, bool RESID, int BY, int PZ, int D, int MINB>
+template <typename T, int STAGE, bool RESID, int BY, int PZ, int D, int MINB, bool CORR = false>
 __global__ void __launch_bounds__(32 * BY, MINB)
     k_substep_march_batch(const SubDev<T>* __restrict__ devs, const int* __restrict__ offs, int n) {
   extern __shared__ __align__(16) double dsm[];
@@ -298,7 +298,7 @@ __global__ void __launch_bounds__(32 * BY, MINB)
   }
   const SubDev<T>& a = devs[lo];
   if (*a.done) return;
-  march_block<T, STAGE, RESID, BY, PZ, D, false>(a, bx - __ldg(offs + lo), dsm, sh, &last);
+  march_block<T, STAGE, RESID, BY, PZ, D, false, CORR>(a, bx - __ldg(offs + lo), dsm, sh, &last);
 }
 
 // Opts the kernel into more than 48 KB of dynamic shared memory, once per
@@ -312,7 +312,7 @@ bool march_opt_in() {
   NRPYELL_CUDA(cudaGetDevice(&dev));
   if (dev >= 0 && dev < 64 && !(devices >> dev & 1ull)) {
     if constexpr (BATCH)
-      NRPYELL_CUDA(cudaFuncSetAttribute(k_substep_march_batch<T, STAGE, RESID, BY, PZ, D, MINB>,
+      NRPYELL_CUDA(cudaFuncSetAttribute(k_substep_march_batch<T, STAGE, RESID, BY, PZ, D, MINB, CORR>,
                                         cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes));
     else
       NRPYELL_CUDA(cudaFuncSetAttribute(k_substep_march<T, STAGE, RESID, BY, PZ, D, MINB, CORR>,
@@ -428,19 +428,19 @@ bool march_stage(int v, const SubstepArgs& a) {
   return false;
 }
 
-template <typename T, int STAGE, bool RESID, int BY, int PZ, int D, int MINB>
+template <typename T, int STAGE, bool RESID, int BY, int PZ, int D, int MINB, bool CORR = false>
 void launch_march_batch_shape(const SubDev<T>* devs, const int* offs, int n, int blocks) {
-  if (!march_opt_in<T, STAGE, RESID, BY, PZ, D, MINB, true>()) return;
-  NRPYELL_LAUNCH_PDL((k_substep_march_batch<T, STAGE, RESID, BY, PZ, D, MINB>), blocks, 32 * BY,
-                     (MarchSmem<T, BY, STAGE, D>::bytes), devs, offs, n);
+  if (!march_opt_in<T, STAGE, RESID, BY, PZ, D, MINB, true, CORR>()) return;
+  NRPYELL_LAUNCH_PDL((k_substep_march_batch<T, STAGE, RESID, BY, PZ, D, MINB, CORR>), blocks, 32 * BY,
+                     (MarchSmem<T, BY, STAGE, D, CORR>::bytes), devs, offs, n);
 }
 
-template <typename T, int STAGE, bool RESID>
+template <typename T, int STAGE, bool RESID, bool CORR = false>
 bool march_batch_stage(int v, const SubDev<T>* devs, const int* offs, int n, int blocks) {
   switch (v) {
-#define NRPYELL_MARCH(I, BY, PZ, D, MINB)                                           \
-  case I:                                                                           \
-    launch_march_batch_shape<T, STAGE, RESID, BY, PZ, D, MINB>(devs, offs, n, blocks); \
+#define NRPYELL_MARCH(I, BY, PZ, D, MINB)                                                 \
+  case I:                                                                                 \
+    launch_march_batch_shape<T, STAGE, RESID, BY, PZ, D, MINB, CORR>(devs, offs, n, blocks); \
     return true;
     NRPYELL_MARCH_SHAPES(NRPYELL_MARCH)
 #undef NRPYELL_MARCH
@@ -526,19 +526,38 @@ template void prepare_march<double>(int);
 template void prepare_march<float>(int);
 
 template <typename T>
-void launch_march_batch(int stage, bool resid, int v, const SubDev<T>* devs, const int* offs, int n, int blocks) {
+void launch_march_batch(int stage, bool resid, int v, const SubDev<T>* devs, const int* offs, int n, int blocks,
+                        bool corr) {
   bool ok = false;
-  switch (stage) {
-    case 1:
-      ok = resid ? march_batch_stage<T, 1, true>(v, devs, offs, n, blocks)
-                 : march_batch_stage<T, 1, false>(v, devs, offs, n, blocks);
-      break;
-    case 2: ok = march_batch_stage<T, 2, false>(v, devs, offs, n, blocks); break;
-    case 3: ok = march_batch_stage<T, 3, false>(v, devs, offs, n, blocks); break;
-    default: ok = march_batch_stage<T, 4, false>(v, devs, offs, n, blocks); break;
+  if (corr) {  // the correction form (FP32 only)
+    if constexpr (sizeof(T) == 4) {
+      switch (stage) {
+        case 1:
+          ok = resid ? march_batch_stage<T, 1, true, true>(v, devs, offs, n, blocks)
+                     : march_batch_stage<T, 1, false, true>(v, devs, offs, n, blocks);
+          break;
+        case 2: ok = march_batch_stage<T, 2, false, true>(v, devs, offs, n, blocks); break;
+        case 3: ok = march_batch_stage<T, 3, false, true>(v, devs, offs, n, blocks); break;
+        default: ok = march_batch_stage<T, 4, false, true>(v, devs, offs, n, blocks); break;
+      }
+    }
+    if (!ok) NRPYELL_FAIL("launch_march_batch: the correction form exists for FP32 only");
+    return;
   }
-  if (!ok) NRPYELL_FAIL("launch_march_batch: no kernel for this shape");
+  if constexpr (sizeof(T) == 8) {  // FP32 batches run the correction form only
+    switch (stage) {
+      case 1:
+        ok = resid ? march_batch_stage<T, 1, true>(v, devs, offs, n, blocks)
+                   : march_batch_stage<T, 1, false>(v, devs, offs, n, blocks);
+        break;
+      case 2: ok = march_batch_stage<T, 2, false>(v, devs, offs, n, blocks); break;
+      case 3: ok = march_batch_stage<T, 3, false>(v, devs, offs, n, blocks); break;
+      default: ok = march_batch_stage<T, 4, false>(v, devs, offs, n, blocks); break;
+    }
+  }
+  if (!ok) NRPYELL_FAIL("launch_march_batch: no kernel for this shape and precision");
 }
-template void launch_march_batch<double>(int, bool, int, const SubDev<double>*, const int*, int, int);
+template void launch_march_batch<double>(int, bool, int, const SubDev<double>*, const int*, int, int, bool);
+template void launch_march_batch<float>(int, bool, int, const SubDev<float>*, const int*, int, int, bool);
 
 }  // namespace nrpyell

@@ -579,13 +579,15 @@ inline SubDev<T> make_dev(const SubstepArgs& a, int by, int p);
 template <typename T>
 bool batch_launch_dev(const SubstepArgs& a, SubDev<T>* out);
 // One substep of n grids; devs (device) holds the grids' arguments for this
-// stage, offs (device) their first block; blocks = total blocks.
+// stage, offs (device) their first block; blocks = total blocks.  corr: the
+// correction form (FP32, marching shapes only; every grid has R0).
 template <typename T>
-void launch_substep_batch(int stage, bool resid, int tile, const SubDev<T>* devs, const int* offs, int n,
-                          int blocks);
+void launch_substep_batch(int stage, bool resid, int tile, const SubDev<T>* devs, const int* offs, int n, int blocks,
+                          bool corr = false);
 // The marching kernel's part of launch_substep_batch: shape v of its list.
 template <typename T>
-void launch_march_batch(int stage, bool resid, int v, const SubDev<T>* devs, const int* offs, int n, int blocks);
+void launch_march_batch(int stage, bool resid, int v, const SubDev<T>* devs, const int* offs, int n, int blocks,
+                        bool corr = false);
 
 template <typename T>
 inline SubDev<T> make_dev(const SubstepArgs& a, int by, int p) {

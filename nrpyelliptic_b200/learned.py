@@ -252,11 +252,12 @@ def compare_solvers(lib, guess, cfgs, log=print):
     from the zero guess -- the plain form -- and from the learned guess with
     the fallback rule (b) one by one in FP64, (c) one by one with the FP32
     correction form of the mixed-precision driver, (d) all together in one
-    batched FP64 relaxation.  Set-up (grids, tables, auxevol) is outside the
-    timings; the learned guess's network evaluation, guess writing and
-    fallback test are inside (b)-(d).  Returns a dict of solves/s, RK4 steps
-    and the speed-up of each form over (a)."""
-    from .batch import relax_batch
+    batched FP64 relaxation, (e) all together with the batched correction
+    form (every step FP32, folded every 256 steps).  Set-up (grids, tables,
+    auxevol) is outside the timings; the learned guess's network evaluation,
+    guess writing and fallback test are inside (b)-(e).  Returns a dict of
+    solves/s, RK4 steps and the speed-up of each form over (a)."""
+    from .batch import relax_batch, relax_batch_mixed
     probs = [Problem(c, lib=lib, host_aux=False, device_tables=True) for c in cfgs]
     states = [DeviceState(p, lib=lib) for p in probs]
     n = len(cfgs)
@@ -276,6 +277,7 @@ def compare_solvers(lib, guess, cfgs, log=print):
         timed_relax(lib, p, ds, False, max_steps=32)
         timed_relax(lib, p, ds, True, max_steps=600)
     relax_batch(probs, states, max_steps=32, lib=lib)
+    relax_batch_mixed(probs, states, fold_every=256, max_steps=32, lib=lib)
     for p, ds in zip(probs, states):
         ds.set_state(p.zero_state())
     t, steps = clock(lambda: [timed_relax(lib, p, ds, False)[0] for p, ds in zip(probs, states)])
@@ -300,8 +302,17 @@ def compare_solvers(lib, guess, cfgs, log=print):
     t, (used, steps, rc) = clock(batched)
     out["batched_fp64_learned"] = {"solves_per_s": n / t, "steps_median": float(np.median(steps)),
                                    "fallbacks": n - int(sum(used)), "not_converged": int(rc)}
+
+    def batched_mixed():
+        used = learned_starts()
+        rc, s32, s64, _, _ = relax_batch_mixed(probs, states, switch=-10.0, fold_every=256, max_steps=40000,
+                                               lib=lib)
+        return used, s32 + s64, rc
+    t, (used, steps, rc) = clock(batched_mixed)
+    out["batched_mixed_learned"] = {"solves_per_s": n / t, "steps_median": float(np.median(steps)),
+                                    "fallbacks": n - int(sum(used)), "not_converged": int(rc)}
     base = out["fp64_zero_guess"]["solves_per_s"]
-    for k in ("fp64_learned", "mixed_learned", "batched_fp64_learned"):
+    for k in ("fp64_learned", "mixed_learned", "batched_fp64_learned", "batched_mixed_learned"):
         out[k]["speedup_vs_fp64_zero_guess"] = out[k]["solves_per_s"] / base
     for ds in states:
         ds.free()
@@ -414,7 +425,7 @@ def main():
     cmp = compare_solvers(lib, guess, test_cfgs)
     T["solver comparison"] = time.perf_counter() - t
     print("\nheld-out solves, one form each (set-up outside the timings):")
-    for k in ("fp64_zero_guess", "fp64_learned", "mixed_learned", "batched_fp64_learned"):
+    for k in ("fp64_zero_guess", "fp64_learned", "mixed_learned", "batched_fp64_learned", "batched_mixed_learned"):
         v = cmp[k]
         print("  %-22s %6.2f solves/s  RK4 steps median %6d  speed-up vs FP64 zero guess %.3f  fallbacks %s"
               % (k, v["solves_per_s"], v["steps_median"], v.get("speedup_vs_fp64_zero_guess", 1.0),

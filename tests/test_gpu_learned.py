@@ -96,3 +96,22 @@ def test_learned_guess_saves_steps_on_held_out_draws(trained):
     assert ev["err_learned"].max() <= 1e-6 and ev["err_mixed"].max() <= 1e-6
     assert fb.sum() <= len(fb) // 2
     assert np.median(ev["steps_learned"]) < np.median(ev["steps_zero"])
+
+
+def test_compare_solvers_every_form_converges(trained):
+    """learned.compare_solvers on held-out draws: the five forms (plain FP64
+    from the zero guess; the learned start with FP64, with the FP32
+    correction form, batched FP64 and batched correction form) all converge,
+    the learned forms take the same fallbacks and median step counts that do
+    not exceed the zero guess's."""
+    from nrpyelliptic_b200.learned import compare_solvers
+    lib, guess, mean, basis, coeffs, hist, energy = trained
+    out = compare_solvers(lib, guess, draws(12, 7003), log=lambda *a: None)
+    forms = ("fp64_learned", "mixed_learned", "batched_fp64_learned", "batched_mixed_learned")
+    print({k: (round(out[k]["solves_per_s"], 2), out[k]["steps_median"]) for k in ("fp64_zero_guess",) + forms})
+    assert len({out[k]["fallbacks"] for k in forms}) == 1
+    for k in ("batched_fp64_learned", "batched_mixed_learned"):
+        assert out[k]["not_converged"] == 0, k
+    for k in forms:
+        assert out[k]["steps_median"] <= out["fp64_zero_guess"]["steps_median"], k
+        assert out[k]["speedup_vs_fp64_zero_guess"] > 0
