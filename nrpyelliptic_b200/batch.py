@@ -2,12 +2,15 @@
 and the seeded sweep command line, on one GPU or sharded by configuration
 over several (one process per GPU, torchrun):
 
-    python -m nrpyelliptic_b200.batch [--n 64] [--seed 20261203] [--tol -10] [--max-steps N]
+    python -m nrpyelliptic_b200.batch [--n 64] [--seed 20261203] [--tol -10] [--max-steps N] [--mixed]
     python -m torch.distributed.run --nproc-per-node 8 --master-addr 127.0.0.1 -m nrpyelliptic_b200.batch
 
 Every RK4 substep of all configurations -- on grids of different sizes -- is
 one kernel launch; sixteen RK4 steps are one CUDA graph, replayed until every
-configuration has reached the tolerance (each stops on its own).
+configuration has reached the tolerance (each stops on its own).  With
+--mixed the sweep runs the FP32 correction form (nrpyell_relax_batch_mixed,
+every step FP32, folded into the FP64 state every 256 steps, the FP64 norm as
+the stop test).
 """
 import argparse
 import ctypes as C
@@ -53,15 +56,20 @@ def relax_batch_mixed(problems, states=None, tol=-10.0, switch=-10.0, fold_every
     return (rc, np.array(s32[:], dtype=np.int64), np.array(s64[:], dtype=np.int64), finals, states)
 
 
-def solve_batch(cfgs, lib=None, tol=-10.0, max_steps=100000, device_tables=True):
+def solve_batch(cfgs, lib=None, tol=-10.0, max_steps=100000, device_tables=True, mixed=False):
     """Set up cfgs (tables and auxevol on the GPU) and relax them together in
-    one batch; per configuration a dict with its RK4 steps, final log10 L2
+    one batch (mixed: the FP32 correction form, every step FP32, fold every
+    256 steps); per configuration a dict with its RK4 steps, final log10 L2
     and a SHA-256 of its converged y_n (ghost zones included)."""
     import hashlib
     lib = lib or _lib.load()
     problems = [Problem(c, lib=lib, host_aux=False, device_tables=device_tables) for c in cfgs]
     states = [DeviceState(p, lib=lib) for p in problems]
-    rc, steps, finals, _ = relax_batch(problems, states, tol, max_steps, lib=lib)
+    if mixed:
+        rc, s32, s64, finals, _ = relax_batch_mixed(problems, states, tol, tol, 256, max_steps, lib=lib)
+        steps = s32 + s64
+    else:
+        rc, steps, finals, _ = relax_batch(problems, states, tol, max_steps, lib=lib)
     out = []
     for c, p, ds, st, f in zip(cfgs, problems, states, steps, finals):
         y = ds.download("y_n")
@@ -103,6 +111,7 @@ def main():
     ap.add_argument("--seed", type=int, default=20261203)
     ap.add_argument("--tol", type=float, default=-10.0)
     ap.add_argument("--max-steps", type=int, default=100000)
+    ap.add_argument("--mixed", action="store_true", help="FP32 correction form (nrpyell_relax_batch_mixed)")
     args = ap.parse_args()
     from .replicas import Replicas
     dist = Replicas()
@@ -111,7 +120,7 @@ def main():
         lib.nrpyell_set_device(dist.local_rank)
         lib.nrpyell_synchronize()  # CUDA context and library stream, outside the timing
         cfgs = sample_sweep(args.n, args.seed)
-        res, sec = sweep(cfgs, dist, lib=lib, tol=args.tol, max_steps=args.max_steps)
+        res, sec = sweep(cfgs, dist, lib=lib, tol=args.tol, max_steps=args.max_steps, mixed=args.mixed)
         if dist.rank == 0:
             print("| config | grid | q | steps | final log10 L2 |")
             print("|---|---|---|---|---|")
@@ -120,9 +129,10 @@ def main():
                 print("| %s | %dx%dx%d | %.2f | %d | %.2f |" % (c.name, *c.Nxx, q, r["steps"], r["final_log10_l2"]))
             pts = sum(r["points"] * r["steps"] for r in res)
             bad = sum(r["final_log10_l2"] > args.tol for r in res)
-            print("\n%d configurations on %d GPU(s), %d not converged; set-up (grids on the host, tables and auxevol "
-                  "on the GPU) and batched relaxation %.2f s (slowest rank) = %.2f solves/s; %.0f Mpoint-RK4-steps/s"
-                  % (len(cfgs), dist.world, bad, sec, len(cfgs) / sec, pts / sec / 1e6))
+            print("\n%d configurations on %d GPU(s)%s, %d not converged; set-up (grids on the host, tables and "
+                  "auxevol on the GPU) and batched relaxation %.2f s (slowest rank) = %.2f solves/s; "
+                  "%.0f Mpoint-RK4-steps/s" % (len(cfgs), dist.world, ", FP32 correction form" if args.mixed else "",
+                                               bad, sec, len(cfgs) / sec, pts / sec / 1e6))
     finally:
         dist.close()
 
