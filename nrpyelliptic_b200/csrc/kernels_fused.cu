@@ -92,8 +92,15 @@ __global__ void __launch_bounds__(32 * BY, MINB) k_substep(SubDev<T> a) {
     const bool y_is_s = STAGE == 1 && a.y == a.S;
     // uu along i2 for planes z0-5 .. z0+P+4 (wrapped by 2 pi)
     T col[P + 10];
+    if (z0 - 5 >= NGHOSTS && z0 + P + 4 < NGHOSTS + Nxx2) {
+      // no plane of the column wraps (uniform over the block)
+      const T* pz = u + (k2 + N01 * (unsigned)(z0 - 5));
 #pragma unroll
-    for (int q = 0; q < P + 10; q++) col[q] = __ldg(u + (k2 + N01 * (unsigned)wrapz(z0 - 5 + q)));
+      for (int q = 0; q < P + 10; q++) col[q] = __ldg(pz + q * N01);
+    } else {
+#pragma unroll
+      for (int q = 0; q < P + 10; q++) col[q] = __ldg(u + (k2 + N01 * (unsigned)wrapz(z0 - 5 + q)));
+    }
     // PF: every pointwise input of the P planes is loaded before the first
     // store (the stores may alias y_n, so the compiler cannot hoist them).
     T pf[8][P];  // unused (and removed) when !PF
