@@ -96,6 +96,7 @@ REAL L2_norm_of_gf_noalloc(const paramstruct *NRPYELL_RESTRICT params, const int
 
 /* Status and error policy. */
 int nrpyell_last_status(void);          /* 0 = ok */
+int nrpyell_gpu_last_status(void);      /* the same status under the harness name a drop-in shim exports */
 const char *nrpyell_last_error(void);
 void nrpyell_clear_status(void);
 void nrpyell_set_exit_on_error(int enable);

@@ -34,6 +34,7 @@ EXPORTS = {
     "L2_norm_of_gf_noalloc": (C.c_double, [P(abi.paramstruct), C.c_int, C.c_double, XX, PREAL]),
     # extensions
     "nrpyell_last_status": (C.c_int, []),
+    "nrpyell_gpu_last_status": (C.c_int, []),
     "nrpyell_last_error": (C.c_char_p, []),
     "nrpyell_clear_status": (None, []),
     "nrpyell_set_exit_on_error": (None, [C.c_int]),

@@ -218,6 +218,7 @@ using namespace nrpyell;
 extern "C" {
 
 int nrpyell_last_status(void) { return g_status; }
+int nrpyell_gpu_last_status(void) { return g_status; }
 const char* nrpyell_last_error(void) { return g_error.c_str(); }
 void nrpyell_clear_status(void) {
   g_status = 0;
