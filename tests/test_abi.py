@@ -69,6 +69,20 @@ def test_status_api_without_gpu_work():
     assert lib.nrpyell_get_step_mode() == 0
 
 
+def test_batched_drivers_reject_empty_batches_without_gpu_work():
+    """n <= 0 or missing arrays: -1 and a recorded error before any CUDA call,
+    under both status names."""
+    lib = _lib.load()
+    for name, args in (("nrpyell_relax_batch", (0, None, None, -10.0, 10, 100.0, None, None)),
+                       ("nrpyell_relax_batch_mixed", (0, None, None, -10.0, -10.0, 256, 10, 100.0, None, None, None))):
+        lib.nrpyell_clear_status()
+        assert getattr(lib, name)(*args) == -1, name
+        assert lib.nrpyell_last_status() != 0 and lib.nrpyell_gpu_last_status() == lib.nrpyell_last_status()
+        assert b"need n > 0" in lib.nrpyell_last_error(), name
+    lib.nrpyell_clear_status()
+    assert lib.nrpyell_gpu_last_status() == 0
+
+
 def test_optimum_eta_damping_formula():
     """Eq. (B6) and (36) of arXiv:2111.02424 as the thorn evaluates them."""
     import math

@@ -110,6 +110,32 @@ def test_batch_mixed_matches_single_mixed_runs(lib, switch, fold, max_steps):
         s.free()
 
 
+def test_batch_mixed_edge_cases(lib):
+    """One configuration equals the single-grid driver; max_steps = 0 takes
+    no step and reports the FP64 norm of the start; a fold_every outside
+    1..4096 is rejected."""
+    from nrpyelliptic_b200.batch import relax_batch_mixed
+    prob = Problem(CONFIGS["shipped_64x64x8"], lib=lib)
+    lib.nrpyell_set_tile(MARCH_8x4)
+    try:
+        rc, s32, s64, finals, states = relax_batch_mixed([prob], tol=-10.0, switch=-6.0, fold_every=100,
+                                                         max_steps=8000, lib=lib)
+        rc1, a32, a64, f1, y1 = _alone_mixed(lib, prob, -6.0, 100, 8000)
+        assert rc == rc1 == 0 and (s32[0], s64[0]) == (a32, a64) and finals[0] == f1
+        np.testing.assert_array_equal(states[0].download("y_n"), y1)
+        states[0].free()
+        rc, s32, s64, finals, states = relax_batch_mixed([prob], tol=-10.0, switch=-10.0, fold_every=100,
+                                                         max_steps=0, lib=lib)
+        assert rc == 1 and s32[0] == 0 and s64[0] == 0 and -8.0 < finals[0] < 0.0
+        assert not np.any(states[0].download("y_n")[:prob.Ntot])
+        for bad in (0, 4097):
+            with pytest.raises(RuntimeError, match="fold_every"):
+                relax_batch_mixed([prob], states, fold_every=bad, max_steps=10, lib=lib)
+        states[0].free()
+    finally:
+        lib.nrpyell_set_tile(-1)
+
+
 def test_batch_autotuned_tile_converges(lib):
     cfgs = [with_grid(c, (32, 32, 8)) for c in sample_sweep(6)]
     probs = [Problem(c, lib=lib) for c in cfgs]
