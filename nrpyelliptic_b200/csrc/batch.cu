@@ -30,6 +30,7 @@ struct BatchWork {
   unsigned int* tickets = nullptr;
   int* offs = nullptr;      // n
   unsigned char* devs = nullptr;  // 5 x n SubDev<T>: stage 1 with stop test, stages 1..4 (tuning uses 2)
+  int* pinned = nullptr;          // host, 2 x n x kStateInts: the polled states of two graph launches
 };
 BatchWork g_batch;
 static_assert(sizeof(SubDev<float>) <= sizeof(SubDev<double>), "batch argument slots hold either precision");
@@ -45,6 +46,7 @@ struct MixedWork {
 MixedWork g_mixed;
 
 void free_batch() {
+  cudaFreeHost(g_batch.pinned);
   cudaFree(g_batch.state);
   cudaFree(g_batch.history);
   cudaFree(g_batch.partials);
@@ -60,6 +62,7 @@ void free_batch() {
 bool ensure_batch(int n, int hist_len, int partials_per) {
   if (g_batch.n >= n && g_batch.hist_len >= hist_len && g_batch.partials_per >= partials_per) return true;
   NRPYELL_CUDA(cudaStreamSynchronize(stream()));
+  cudaFreeHost(g_batch.pinned);
   cudaFree(g_batch.state);
   cudaFree(g_batch.history);
   cudaFree(g_batch.partials);
@@ -77,6 +80,7 @@ bool ensure_batch(int n, int hist_len, int partials_per) {
   NRPYELL_CUDA(dev_alloc(&g_batch.offs, sizeof(int) * n));
   NRPYELL_CUDA(dev_alloc(&g_batch.devs, sizeof(SubDev<double>) * 5 * n));
   NRPYELL_CUDA(cudaMemset(g_batch.tickets, 0, sizeof(unsigned int) * n));
+  NRPYELL_CUDA(cudaMallocHost(&g_batch.pinned, sizeof(int) * kStateInts * n * 2));
   return status_ok();
 }
 
@@ -229,8 +233,7 @@ bool run_batch(const std::vector<Grid>& gs, bool corr, int* tile, BatchResult* o
 
   // replay until every grid is done, polling the states of launch k-1
   // while launch k runs
-  int* pinned = nullptr;
-  NRPYELL_CUDA(cudaMallocHost(&pinned, sizeof(int) * kStateInts * n * 2));
+  int* pinned = g_batch.pinned;
   cudaEvent_t ev[2];
   NRPYELL_CUDA(cudaEventCreateWithFlags(&ev[0], cudaEventDisableTiming));
   NRPYELL_CUDA(cudaEventCreateWithFlags(&ev[1], cudaEventDisableTiming));
@@ -256,7 +259,6 @@ bool run_batch(const std::vector<Grid>& gs, bool corr, int* tile, BatchResult* o
   cudaEventDestroy(ev[1]);
   std::vector<int> st(kStateInts * n);
   NRPYELL_CUDA(cudaMemcpy(st.data(), g_batch.state, sizeof(int) * kStateInts * n, cudaMemcpyDeviceToHost));
-  cudaFreeHost(pinned);
   if (!status_ok()) return false;
   out->steps.assign(n, 0);
   out->converged.assign(n, 0);
