@@ -315,7 +315,7 @@ int nrpyell_relax_batch(int n, griddata_struct *grids, const REAL *dt, REAL log1
  * batches (marching shapes for the FP32 stretches).  With the same tile
  * shapes each configuration's result is bitwise that of nrpyell_relax_mixed.
  * steps_fp32[c], steps_fp64[c], final_log10_l2[c] as there (each array may
- * be NULL); the FP32 buffers (15 Ntot floats per configuration) stay
+ * be NULL); the FP32 buffers (13 Ntot floats per configuration) stay
  * allocated for later calls until nrpyell_release_tables.  Returns the number
  * of configurations that did not converge, < 0 on error. */
 int nrpyell_relax_batch_mixed(int n, griddata_struct *grids, const REAL *dt, REAL log10_tol, REAL log10_switch,

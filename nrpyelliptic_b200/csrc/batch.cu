@@ -371,7 +371,7 @@ extern "C" int nrpyell_relax_batch_mixed(const int n, griddata_struct* grids, co
       return -1;
     }
     off[c] = floats;
-    floats += 6 * 2 * (size_t)gs[c].d.Ntot + 3 * (size_t)gs[c].d.Ntot;
+    floats += 5 * 2 * (size_t)gs[c].d.Ntot + 3 * (size_t)gs[c].d.Ntot;
     max_tiles = std::max(max_tiles, max_interior_blocks(gs[c].d));
   }
   if (g_mixed.floats < floats || g_mixed.n < n) {

@@ -650,7 +650,7 @@ int nrpyell_relax_mixed(griddata_struct* g, const REAL dt, const REAL log10_tol,
   const Dims d = su.d;
   const long long n2 = 2 * d.Ntot;
   FusedWork* w = su.w;
-  if (!w->f32) NRPYELL_CUDA(dev_alloc(&w->f32, sizeof(float) * (6 * n2 + 3 * d.Ntot)));
+  if (!w->f32) NRPYELL_CUDA(dev_alloc(&w->f32, sizeof(float) * (5 * n2 + 3 * d.Ntot)));
   const int cycle_len = std::min(fold_every, max_steps);
   if (!w->cycle_history) NRPYELL_CUDA(dev_alloc(&w->cycle_history, sizeof(double) * (kMaxFoldEvery + 1)));
   if (!status_ok()) return -1;
