@@ -120,8 +120,9 @@ SubstepArgs substep_args(const Dims& d, RfmTables* rt, BcTables* bt, Scratch* s,
 // and keeps the fastest, once per grid size and precision (and form).  Each
 // shape is timed on whole RK4 steps as the relaxation runs them -- stage 1
 // storing its residual partials when an L2 table is given (the per-tile
-// reduction depends on the shape), then stages 2, 3 and 4 -- one warm-up
-// step and the best of three 4-step timings.  Stage 4 writes y_n, so y_n is
+// reduction depends on the shape) and the stop test's reduction forked
+// beside stage 2 and joined before stage 3, then stages 2, 3 and 4 -- one
+// warm-up step and the best of five 8-step timings.  Stage 4 writes y_n, so y_n is
 // saved before the timings and restored after them.
 template <typename T>
 int tuned_tile(const Dims& d, RfmTables* rt, BcTables* bt, FusedWork* w, Scratch* sc, const StateBuffers& b,
@@ -147,15 +148,28 @@ int tuned_tile(const Dims& d, RfmTables* rt, BcTables* bt, FusedWork* w, Scratch
     for (int st = 1; st <= 4; st++) a[st - 1] = substep_args(d, rt, bt, sc, b, rp, st, w->zero_flag, w->state, t);
     if (lt) {
       a[0].lt = lt;
-      a[0].defer_l2 = 1;  // partials only, as in relax_loop (no stop test here)
+      a[0].defer_l2 = 1;  // partials only, reduced beside stage 2 as in relax_loop
     }
+    // one RK4 step as relax_loop runs it: with an L2 table the stop test's
+    // reduction is forked after stage 1 and joined before stage 3 (its
+    // state is w->state, which relax_loop resets before every relaxation;
+    // the kernels here wait on w->zero_flag, so they always run)
+    auto step = [&]() {
+      launch_substep<T>(1, a[0]);
+      if (lt) launch_finalize_forked<T>(a[0]);
+      for (int st = 2; st <= 4; st++) {
+        if (lt && st == 3) join_finalize();
+        launch_substep<T>(st, a[st - 1]);
+      }
+    };
     prepare_substep<T>(t);
-    for (int st = 1; st <= 4; st++) launch_substep<T>(st, a[st - 1]);
+    step();
+    // best of five 8-step timings: the leading one-plane shapes at
+    // 128x128x16 differ by 0.5-2 %, within the noise of shorter timings
     float tmin = 1e30f;
-    for (int rep = 0; rep < 3; rep++) {
+    for (int rep = 0; rep < 5; rep++) {
       NRPYELL_CUDA(cudaEventRecord(e0, stream()));
-      for (int i = 0; i < 4; i++)
-        for (int st = 1; st <= 4; st++) launch_substep<T>(st, a[st - 1]);
+      for (int i = 0; i < 8; i++) step();
       NRPYELL_CUDA(cudaEventRecord(e1, stream()));
       NRPYELL_CUDA(cudaEventSynchronize(e1));
       float ms = 0.0f;
