@@ -5,13 +5,14 @@ uu_rhs = vv - eta uu).  The guess is used only when its residual L2 is below
 the zero guess's (else the zero guess is the fallback), and the FP64
 relaxation from either start decides the final error.
 
-    python -m nrpyelliptic_b200.learned [--train 4096] [--test 256] [--modes 256] [--epochs 400]
+    python -m nrpyelliptic_b200.learned [--train 4096] [--test 256] [--modes 256] [--epochs 400] [--mixed-training]
     python -m nrpyelliptic_b200.learned --mlp-only [--epochs 5]   (network training throughput)
 
 Pipeline (one GPU):
   1. training solves: `--train` configurations drawn from the seeded sweep
      distribution (sample_sweep) on the 128x128x16 grid, relaxed from the
-     zero guess to log10 L2 <= -10 in batches (nrpyell_relax_batch);
+     zero guess to log10 L2 <= -10 in batches (nrpyell_relax_batch, or with
+     --mixed-training the batched FP32 correction form);
   2. POD by the method of snapshots on the host (float32 Gram matrix of the
      centred uu snapshots, float64 eigendecomposition), `--modes` modes;
   3. MLP 13 -> 4 x 512 (tanh) -> modes, trained with the library's BF16
@@ -30,7 +31,7 @@ import time
 import numpy as np
 
 from . import _lib
-from .batch import relax_batch
+from .batch import relax_batch, relax_batch_mixed
 from .problem import DeviceState, Problem, sample_sweep, with_grid
 
 GRID = (128, 128, 16)
@@ -47,16 +48,21 @@ def configs(n, seed):
     return [with_grid(c, GRID) for c in sample_sweep(n, seed)]
 
 
-def solve_snapshots(cfgs, lib, chunk=64, tol=-10.0, max_steps=40000, log=print, dist=None):
+def solve_snapshots(cfgs, lib, chunk=64, tol=-10.0, max_steps=40000, log=print, dist=None, mixed=False):
     """Relax every configuration from the zero guess in batches; returns the
     converged uu arrays (float32, ghost zones included) and step counts.
+    mixed: the batched FP32 correction form (every step FP32, folded into the
+    FP64 state every 256 steps, the FP64 norm as the stop test) instead of
+    the FP64 batch; the snapshots then differ from the FP64 ones by ~1e-8 of
+    max|uu|, far below what a POD basis resolves.
     With `dist` (replicas.Replicas, one process per GPU) the configurations
     are dealt round-robin over the ranks, each rank solves its share, and the
     snapshots are gathered on the host of every rank."""
     if dist is not None and dist.world > 1:
         from .replicas import shard
         mine = shard(list(range(len(cfgs))), dist.rank, dist.world)
-        part = solve_snapshots([cfgs[i] for i in mine], lib, chunk, tol, max_steps, log) if mine else (None, [])
+        part = (solve_snapshots([cfgs[i] for i in mine], lib, chunk, tol, max_steps, log, mixed=mixed) if mine
+                else (None, []))
         parts = dist.all_gather((mine, part[0], list(part[1])))
         ntot = next(p[1].shape[1] for p in parts if p[1] is not None)
         snaps = np.empty((len(cfgs), ntot), np.float32)
@@ -69,7 +75,12 @@ def solve_snapshots(cfgs, lib, chunk=64, tol=-10.0, max_steps=40000, log=print, 
     snaps, steps = None, []
     for c0 in range(0, len(cfgs), chunk):
         probs = [Problem(c, lib=lib, host_aux=False, device_tables=True) for c in cfgs[c0:c0 + chunk]]
-        rc, st, _, states = relax_batch(probs, tol=tol, max_steps=max_steps, lib=lib)
+        if mixed:
+            rc, s32, s64, _, states = relax_batch_mixed(probs, tol=tol, switch=tol, fold_every=256,
+                                                        max_steps=max_steps, lib=lib)
+            st = s32 + s64
+        else:
+            rc, st, _, states = relax_batch(probs, tol=tol, max_steps=max_steps, lib=lib)
         if snaps is None:
             snaps = np.empty((len(cfgs), probs[0].Ntot), np.float32)
         for i, (p, s) in enumerate(zip(probs, states)):
@@ -380,6 +391,8 @@ def main():
     ap.add_argument("--epochs", type=int, default=400)
     ap.add_argument("--seed", type=int, default=20261203)
     ap.add_argument("--test-seed", type=int, default=20261204)
+    ap.add_argument("--mixed-training", action="store_true",
+                    help="training solves with the batched FP32 correction form (nrpyell_relax_batch_mixed)")
     ap.add_argument("--dump", default=None, help="write the regression data (features, POD coefficients) to this .npz")
     ap.add_argument("--mlp-only", action="store_true",
                     help="time the network's training on synthetic data only (no solves)")
@@ -393,7 +406,7 @@ def main():
     T = {}
     t = time.perf_counter()
     train_cfgs = configs(args.train, args.seed)
-    snaps, steps = solve_snapshots(train_cfgs, lib)
+    snaps, steps = solve_snapshots(train_cfgs, lib, mixed=args.mixed_training)
     T["training solves"] = time.perf_counter() - t
     print("training solves: %d, RK4 steps median %d" % (len(steps), int(np.median(steps))))
     t = time.perf_counter()

@@ -115,3 +115,17 @@ def test_compare_solvers_every_form_converges(trained):
     for k in forms:
         assert out[k]["steps_median"] <= out["fp64_zero_guess"]["steps_median"], k
         assert out[k]["speedup_vs_fp64_zero_guess"] > 0
+
+
+def test_mixed_training_solves_match_fp64_snapshots():
+    """solve_snapshots with the batched FP32 correction form: every draw
+    converges within one RK4 step of the FP64 batch, and its snapshot differs
+    from the FP64 one by at most 1e-6 of max|uu| (far below the POD error)."""
+    lib = _lib.load()
+    cfgs = draws(8, 7004)
+    s64, n64 = solve_snapshots(cfgs, lib, chunk=8, log=lambda *a: None)
+    s32, n32 = solve_snapshots(cfgs, lib, chunk=8, log=lambda *a: None, mixed=True)
+    assert np.all(np.abs(n32 - n64) <= 1), (n32, n64)
+    err = np.max(np.abs(s32.astype(np.float64) - s64), axis=1) / np.max(np.abs(s64), axis=1)
+    print("mixed training snapshots: steps %s vs %s, max rel diff %.2e" % (list(n32), list(n64), err.max()))
+    assert err.max() <= 1e-6
